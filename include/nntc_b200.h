@@ -1,0 +1,238 @@
+/* nntc_b200.h: the C ABI of the B200-native encoder hot path.
+ *
+ * Every entry point here stands in for one function of the reference's device seam. The reference declares those as
+ * 46 C++ functions over `DeviceModel*` (src/cuda_backend.h:20-80, which is src/backend.h:86-150 with DeviceModel* in
+ * place of be::Device*); their C++ signatures carry std::vector, std::string and Model&, which no FFI can bind. This
+ * header restates each one over plain pointers and sizes:
+ *
+ *   - the reference's `Model` (src/model.h:56-114) becomes `nntc_b200_model`, a fixed-size POD carrying the layout,
+ *     the decoder, the per-output weights and the grids. The per-plane arrays Model owns (k0, k1, the BC blocks) are
+ *     passed as caller-owned per-plane buffers, one pointer per stored plane, sized by the layout;
+ *   - the report structs (Level1Report, Level0Report, Objective, BcRefineReport, Level1InitReport,
+ *     Init0ChannelReport, src/model.h:281-519) become fixed-size PODs with the same fields;
+ *   - every call returns an int status (NNTC_B200_OK on success) instead of printing and exiting; the message of the
+ *     last failure is nntc_b200_last_error(). The C++ adapter in nntc_b200/seam turns a failure back into the
+ *     reference's one ERROR line and exit status 1 (src/device.cuh:45-76).
+ *
+ * Threading: one host thread per device handle. Every call returns with its results visible to the host, as the
+ * reference's calls do (each block ends with one synchronisation of the master stream, src/device.cuh:403-411).
+ */
+#ifndef NNTC_B200_H
+#define NNTC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NNTC_B200_MAX_PLANES 13    /* the base and MAX_MIP_LEVELS = 12 more (src/model.h:32) */
+#define NNTC_B200_MAX_CHANNELS 4   /* per-level channel cap (src/device.cuh:80) */
+#define NNTC_B200_MAX_NIN 24       /* |phi| cap (src/device.cuh:81) */
+#define NNTC_B200_MAX_NOUT 18      /* 3 channels x MAX_TEXTURES 6 (src/model.h:39, src/device.cuh:82) */
+
+enum nntc_b200_status
+{
+    NNTC_B200_OK = 0,
+    NNTC_B200_ERR_ARG = 1,     /* an argument the call cannot take (a size, a plane index, a null pointer) */
+    NNTC_B200_ERR_CUDA = 2,    /* a CUDA call failed; the message names it */
+    NNTC_B200_ERR_OOM = 3,     /* device memory ran out (src/init.cu:135-149 says it in the user's terms) */
+    NNTC_B200_ERR_NODEV = 4,   /* no usable device */
+    NNTC_B200_ERR_STATE = 5,   /* the call needs state the handle does not have (e.g. level 0's grid outside bc8) */
+    NNTC_B200_ERR_TIMEOUT = 6  /* a bounded device-side wait gave up; the device status word says where */
+};
+
+/* The model: src/model.h:56-114 as a fixed-size POD. Fields that are std::vector in the reference carry a count. */
+typedef struct nntc_b200_model
+{
+    int textures;                 /* T */
+    int nout;                     /* 3 T */
+    int width, height;            /* level 0's base extent */
+    int c0, c1;                   /* level-0 and level-1 channels */
+    int bits0[NNTC_B200_MAX_CHANNELS];
+    int bits1;
+    int bc0;                      /* the shipped level-0 format is BC4/BC5 (decides the palette) */
+    int l0_bc8;                   /* --l0 bc8: level 0 is a continuous 8-bit plane on lo0/hi0 */
+    int init0_residual, init0_texture, init0_chain;
+    int nin;                      /* C1 + C0 + C0 C1 */
+    int nplanes;                  /* the base first */
+    int w0[NNTC_B200_MAX_PLANES], h0[NNTC_B200_MAX_PLANES];
+    int w1[NNTC_B200_MAX_PLANES], h1[NNTC_B200_MAX_PLANES];
+    float cw[NNTC_B200_MAX_NOUT]; /* per-output weight of the objective */
+    int has_decoder;              /* 0: m.dec.w / m.dec.b are empty (no decoder yet) */
+    float dec_w[NNTC_B200_MAX_NOUT * NNTC_B200_MAX_NIN];   /* nout x nin, row-major */
+    float dec_b[NNTC_B200_MAX_NOUT];
+    int palette0_len[NNTC_B200_MAX_CHANNELS];              /* 0 under --l0 bc8 */
+    float palette0[NNTC_B200_MAX_CHANNELS][16];
+    int has_lo0, has_lo1;         /* lo0/hi0 and lo1/hi1 present (non-empty vectors in the reference) */
+    float lo0[NNTC_B200_MAX_CHANNELS], hi0[NNTC_B200_MAX_CHANNELS];
+    float lo1[NNTC_B200_MAX_CHANNELS], hi1[NNTC_B200_MAX_CHANNELS];
+} nntc_b200_model;
+
+typedef struct nntc_b200_device_info
+{
+    char name[256];
+    int major, minor;
+    char error[512];
+} nntc_b200_device_info;
+
+/* Level1Report, src/model.h:374-398. */
+typedef struct nntc_b200_plane_report
+{
+    int iterations;
+    double residual, lambda, min_diag, max_diag;
+    double ms_assemble, ms_precond, ms_cg;
+    long long moved_values;
+    double delta2, plane2;
+    float lo[NNTC_B200_MAX_CHANNELS], hi[NNTC_B200_MAX_CHANNELS];
+    int quantised, sweeps;
+    long long moved;
+    double ms_sweeps;
+} nntc_b200_plane_report;
+
+/* Level0Report, src/model.h:440-447. */
+typedef struct nntc_b200_level0_report
+{
+    long long moved[4];
+    long long moved_total;
+    double ms;
+    int joint;
+    long long states;
+} nntc_b200_level0_report;
+
+/* Objective, src/model.h:467-478, with the per-plane vectors as fixed arrays of nplanes entries. */
+typedef struct nntc_b200_objective
+{
+    double e;
+    double e_plane[NNTC_B200_MAX_PLANES];
+    double centre_mse, sampled_mse;
+    double centre_plane[NNTC_B200_MAX_PLANES];
+    double ms;
+} nntc_b200_objective;
+
+/* Level1InitReport, src/model.h:281-289. */
+typedef struct nntc_b200_init1_report
+{
+    int pca, components;
+    double eigenvalue[4], peak[4];
+    double total_variance;
+} nntc_b200_init1_report;
+
+/* Init0ChannelReport, src/model.h:314-326. */
+typedef struct nntc_b200_init0_report
+{
+    double eigenvalue, total_variance, share, peak, divisor;
+    double dir[NNTC_B200_MAX_NOUT];
+    int nout, texture;
+} nntc_b200_init0_report;
+
+/* BcRefineReport, src/model.h:512-519. */
+typedef struct nntc_b200_bc_report
+{
+    int pass;
+    long long blocks, improved;
+    double delta_e, ms;
+} nntc_b200_bc_report;
+
+typedef struct nntc_b200_device nntc_b200_device;
+
+/* The message of the last failed call on this thread; "" when none failed. */
+const char* nntc_b200_last_error(void);
+/* 1 when this library was built for the device it finds (sm_100a kernels), else 0. */
+int nntc_b200_version(void);
+
+/* ---- lifecycle: src/init.cu:76-382 (device_select, device_create, device_destroy, device_memory) ---- */
+int nntc_b200_device_select(int index, nntc_b200_device_info* info);           /* returns 1 if usable */
+int nntc_b200_device_create(const nntc_b200_model* m, const float* const* source_chain, nntc_b200_device** out);
+void nntc_b200_device_destroy(nntc_b200_device* d);                             /* NULL is a no-op */
+size_t nntc_b200_device_memory(const nntc_b200_device* d);
+
+/* ---- initialisation and grids: src/init.cu:446-1400 ---- */
+int nntc_b200_init_level0(nntc_b200_device* d, const nntc_b200_model* m, const float luma[3], int luma_channel0,
+                          uint8_t* const* k0_out);
+int nntc_b200_init_level1(nntc_b200_device* d, nntc_b200_model* m, int pca, nntc_b200_init1_report* rep,
+                          uint8_t* const* k1_out);
+int nntc_b200_init0_residual_channel(nntc_b200_device* d, const nntc_b200_model* m, int channel,
+                                     const double* plane_weight, nntc_b200_init0_report* rep, uint8_t* const* k0_io);
+/* range_pct: 1 for --q1-range pct, 0 for minmax. lo/hi written into m, indices into k_out. */
+int nntc_b200_quantise_level1(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k1_out);
+int nntc_b200_freeze_level1_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k1_out);
+int nntc_b200_quantise_level0(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out);
+int nntc_b200_freeze_level0_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out);
+int nntc_b200_snap_level0_on_grid(nntc_b200_device* d, const nntc_b200_model* m, uint8_t* const* k0_out);
+int nntc_b200_stencil_monomials(int c0);
+
+/* ---- block (a): src/solve_decoder.cu:267-458. m->dec_w / dec_b / has_decoder are read and written. ---- */
+int nntc_b200_solve_decoder(nntc_b200_device* d, nntc_b200_model* m, int k, const double* per_site, double* ms);
+void nntc_b200_decoder_ridge_tally(long long out[4]);
+
+/* ---- blocks (b) and (c'): src/solve_level1.cu:1222-1449. rep holds m->nplanes entries. ---- */
+int nntc_b200_solve_level1_all(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
+                               nntc_b200_plane_report* rep, double* ms);
+int nntc_b200_sweep_level1_all(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int sweeps,
+                               nntc_b200_plane_report* rep, double* ms);
+int nntc_b200_solve_level0_cont_all(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
+                                    nntc_b200_plane_report* rep, double* ms);
+int nntc_b200_sweep_level0_cont_all(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int sweeps,
+                                    nntc_b200_plane_report* rep, double* ms);
+int nntc_b200_assemble_level0_for_refine(nntc_b200_device* d, const nntc_b200_model* m, int k, double* ms);
+
+/* ---- transfers: src/solve_level1.cu:1098-1500, src/solve_level0.cu:329-369. A size that does not match the plane
+ * is silently ignored on upload, as the reference's uploads do (src/solve_level1.cu:1478-1479). ---- */
+int nntc_b200_level1_download_indices(nntc_b200_device* d, int plane, uint8_t* k1, size_t n);
+int nntc_b200_level1_upload(nntc_b200_device* d, int plane, const float* v1, size_t n);
+int nntc_b200_level1_upload_indices(nntc_b200_device* d, int plane, const uint8_t* k1, size_t n);
+int nntc_b200_level0_upload_indices(nntc_b200_device* d, int plane, const uint8_t* k0, size_t n);
+int nntc_b200_upload_decoder(nntc_b200_device* d, const nntc_b200_model* m);
+int nntc_b200_upload_grids(nntc_b200_device* d, const nntc_b200_model* m);
+int nntc_b200_level1_download(nntc_b200_device* d, int plane, float* v1, size_t n);
+int nntc_b200_level1_delta(nntc_b200_device* d, int plane, double* delta, size_t n);
+int nntc_b200_level1_poke(nntc_b200_device* d, int plane, size_t index, float value);
+int nntc_b200_level1_range(nntc_b200_device* d, int plane, float* lo, float* hi);
+int nntc_b200_solve_level1_dense_host(nntc_b200_device* d, const nntc_b200_model* m, int k, int plane, double lambda,
+                                      const float* c_prev, size_t n_prev, double* delta, int max_unknowns);
+int nntc_b200_level0_download(nntc_b200_device* d, int plane, uint8_t* k0, size_t n);
+int nntc_b200_level0_upload(nntc_b200_device* d, int plane, const float* v0, size_t n);
+int nntc_b200_level0_download_values(nntc_b200_device* d, int plane, float* v0, size_t n);
+
+/* ---- block (c), palette mode: src/solve_level0.cu:275-327. k0 host mirror written per plane. ---- */
+int nntc_b200_solve_level0_all(nntc_b200_device* d, const nntc_b200_model* m, int k, int sweeps,
+                               nntc_b200_level0_report* rep, double* ms);
+
+/* ---- the objective and the decode: src/objective.cu:53-380 ---- */
+int nntc_b200_decode_plane(nntc_b200_device* d, const nntc_b200_model* m, int plane, uint8_t* rgb8, size_t n);
+int nntc_b200_objective_eval(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                             nntc_b200_objective* r);
+double nntc_b200_objective_total_ms(void);
+long long nntc_b200_objective_passes(void);
+int nntc_b200_objective_check_host(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                                   nntc_b200_objective* r);
+
+/* ---- the BC refinement: src/refine_bc.cu:504-644. ep / sel are per-plane buffers of blocks*C0*2 and blocks*C0*16
+ * bytes (block-major, then channel), exactly as the reference holds them. k0_host is the model's k0 mirror (what
+ * the seed pack reads, src/export.cpp:294-328). ---- */
+int nntc_b200_bc_pack_prepare(nntc_b200_device* d, const nntc_b200_model* m, int k, int seed,
+                              const uint8_t* const* k0_host, double* ms);
+int nntc_b200_bc_refine(nntc_b200_device* d, const nntc_b200_model* m, int passes, nntc_b200_bc_report* rep,
+                        double* ms);
+int nntc_b200_bc_state_save(nntc_b200_device* d, const nntc_b200_model* m, uint8_t* const* ep, uint8_t* const* sel);
+int nntc_b200_bc_state_restore(nntc_b200_device* d, const nntc_b200_model* m, const uint8_t* const* ep,
+                               const uint8_t* const* sel);
+/* The .dds block bytes of one plane from ep/sel (src/export.cpp:333-370, shared/bc_pack.h:74-85), and the pack's
+ * squared error in byte units against k0's exact index values, ADDED to *se and *n. files[f] holds
+ * blocks * (nc == 1 ? 8 : 16) bytes for file f (one file for 1-2 channels, two for 3-4). */
+int nntc_b200_bc_pack_blocks(const nntc_b200_model* m, int plane, const uint8_t* ep, const uint8_t* sel,
+                             const uint8_t* k0, uint8_t* const* files, double* se, size_t* n);
+
+/* ---- probes: what the reference's per-kernel harness reads (src/backend_check_probe.h:20-37) ---- */
+int nntc_b200_probe_normal_equations(nntc_b200_device* d, double* out, size_t n);
+int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double* stencil, double* grad,
+                              float* precond, double* cg_x, float* prev);
+int nntc_b200_probe_monomials(nntc_b200_device* d, int level0, double* out, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NNTC_B200_H */

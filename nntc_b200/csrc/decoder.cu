@@ -1,0 +1,427 @@
+// decoder.cu: block (a), the decoder as one global least squares (src/solve_decoder.cu:1-458).
+//
+// With v = [phi ; 1] (mm = nin + 1) and the target t, the normal equations are A = sum omega v v^T (upper triangle)
+// and rhs_c = sum omega v t_c; W and b follow by Gauss-Jordan with the ridge ladder {1e-9, 1e-12, 0} mean(diag A)
+// and the acceptance test on the objective's own quadratic Q (src/solve_decoder.cu:184-458), on the host.
+//
+// The accumulation, B200 shape. Every product is a float times a float, which is EXACT in double, so what matters
+// for throughput is how many shared-memory operands feed each DFMA. The reference walks the 775 entries one dot
+// product per thread (two shared loads per multiply-add). Here a block stages 256 sites' [v | t] in shared memory and
+// each thread owns a 4x4 TILE of X^T X (X = [v | t]) over a k-slice of the staged sites: 8 loads feed 16 DFMAs. Only
+// the tiles the system needs are computed: the upper triangle of V^T V and all of T^T V. Every plane of the chain is
+// in the one launch (grid.y is the plane). Each block keeps its tiles in registers over all of its chunks, folds its
+// k-slices in a fixed order and writes one partial per entry; a second kernel adds, per entry, the planes in index
+// order with their site weight omega and the blocks in index order (src/solve_decoder.cu:165-180): deterministic.
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "device.cuh"
+
+namespace nb
+{
+
+constexpr int LS_THREADS = 256;
+constexpr int LS_GRID = 148 * 2;   // blocks per plane
+constexpr int TILE = 4;
+constexpr int LS_STRIDE = LS_THREADS + 1;
+constexpr int VP_MAX = (MAX_NIN + 1 + TILE - 1) / TILE * TILE;   // 28
+constexpr int TP_MAX = (MAX_NOUT + TILE - 1) / TILE * TILE;      // 20
+
+__host__ __device__ inline int tri_index(int i, int j, int mm)
+{
+    return i * mm - i * (i - 1) / 2 + (j - i);
+}
+
+// The tiles a launch computes: (row tile, col tile) with row tiles 0..nv-1 over V (upper triangle, col >= row) and
+// nv..nv+nt-1 over T (every col tile of V).
+struct LsShape
+{
+    int mm, nout, nv, nt, tiles, ks;
+    int trow[64], tcol[64];
+};
+
+inline LsShape ls_shape(int nin, int nout)
+{
+    LsShape s{};
+    s.mm = nin + 1;
+    s.nout = nout;
+    s.nv = (s.mm + TILE - 1) / TILE;
+    s.nt = (nout + TILE - 1) / TILE;
+    int n = 0;
+    for (int i = 0; i < s.nv; i++)
+        for (int j = i; j < s.nv; j++)
+        {
+            s.trow[n] = i;
+            s.tcol[n] = j;
+            n++;
+        }
+    for (int i = 0; i < s.nt; i++)
+        for (int j = 0; j < s.nv; j++)
+        {
+            s.trow[n] = s.nv + i;
+            s.tcol[n] = j;
+            n++;
+        }
+    s.tiles = n;
+    s.ks = LS_THREADS / n;   // k-slices of the staged chunk
+    return s;
+}
+
+struct LsArgs
+{
+    double* partial;   // [plane][entry][LS_GRID]
+    int entries;
+};
+
+__global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape S, LsArgs A)
+{
+    extern __shared__ double ls_sh[];
+    double* fold = ls_sh;                              // LS_THREADS doubles
+    float* sx = (float*)(ls_sh + LS_THREADS);          // [col][site]: V columns 0..VP-1, then T columns
+    const int pl = blockIdx.y;
+    const PlaneView& V = P.p[pl];
+    const int c0 = P.c0, c1 = P.c1, nin = P.nin, nout = P.nout, kc = P.kc, mm = S.mm;
+    const int VP = S.nv * TILE, TP = S.nt * TILE;
+    const int per_pixel = 1 + kc;
+    const size_t sites = (size_t)V.w0 * V.h0 * per_pixel;
+    const size_t chunks = (sites + LS_THREADS - 1) / LS_THREADS;
+    const int tid = threadIdx.x;
+    const int tile = tid % S.tiles, kg = tid / S.tiles;
+    const bool worker = kg < S.ks;
+    const int r0 = S.trow[tile] * TILE, cc0 = S.tcol[tile] * TILE;   // row in [V|T] column space, col in V
+    double acc[TILE][TILE];
+    for (int a = 0; a < TILE; a++)
+        for (int b = 0; b < TILE; b++)
+            acc[a][b] = 0.0;
+
+    for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
+    {
+        const size_t si = chunk * LS_THREADS + tid;
+        float phi[MAX_NIN], tgt[MAX_NOUT];
+        float one = 0.0f;
+        for (int i = 0; i < nin; i++)
+            phi[i] = 0.0f;
+        for (int c = 0; c < nout; c++)
+            tgt[c] = 0.0f;
+        if (si < sites)
+        {
+            const size_t pixel = si / (size_t)per_pixel;
+            const int j = (int)(si % (size_t)per_pixel);
+            const int px = (int)(pixel % (size_t)V.w0), py = (int)(pixel / (size_t)V.w0);
+            float dx, dy;
+            site_offset(kc, j, px, py, dx, dy);
+            float s[MAX_CH], c[MAX_CH];
+            const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
+            blend<MAX_CH>(V.v1, V.w1, c1, t1, c);
+            if (j == 0)
+            {
+                for (int i = 0; i < c0; i++)
+                    s[i] = V.v0[pixel * c0 + i];
+                for (int i = 0; i < nout; i++)
+                    tgt[i] = __ldg(V.src + pixel * nout + i);
+            }
+            else
+            {
+                const Tap t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+                blend<MAX_CH>(V.v0, V.w0, c0, t0, s);
+                blend<MAX_NOUT>(V.src, V.w0, nout, t0, tgt);
+            }
+            features(s, c0, c, c1, phi);
+            one = 1.0f;
+        }
+        __syncthreads();   // the previous chunk's tiles have finished reading
+        for (int i = 0; i < nin; i++)
+            sx[i * LS_STRIDE + tid] = phi[i];
+        sx[nin * LS_STRIDE + tid] = one;
+        for (int i = mm; i < VP; i++)
+            sx[i * LS_STRIDE + tid] = 0.0f;
+        for (int c = 0; c < nout; c++)
+            sx[(VP + c) * LS_STRIDE + tid] = tgt[c];
+        for (int c = nout; c < TP; c++)
+            sx[(VP + c) * LS_STRIDE + tid] = 0.0f;
+        __syncthreads();
+        if (worker)
+        {
+            const float* rowp = sx + r0 * LS_STRIDE;
+            const float* colp = sx + cc0 * LS_STRIDE;
+            for (int p = kg; p < LS_THREADS; p += S.ks)
+            {
+                double a[TILE], b[TILE];
+                for (int q = 0; q < TILE; q++)
+                {
+                    a[q] = (double)rowp[q * LS_STRIDE + p];
+                    b[q] = (double)colp[q * LS_STRIDE + p];
+                }
+                for (int x = 0; x < TILE; x++)
+                    for (int y = 0; y < TILE; y++)
+                        acc[x][y] = fma(a[x], b[y], acc[x][y]);
+            }
+        }
+    }
+
+    // Fold the k-slices in order 0..ks-1, entry by entry, and write the entries this tile owns.
+    for (int x = 0; x < TILE; x++)
+        for (int y = 0; y < TILE; y++)
+        {
+            __syncthreads();
+            fold[tid] = acc[x][y];
+            __syncthreads();
+            if (worker && kg == 0)
+            {
+                double s = 0.0;
+                for (int g = 0; g < S.ks; g++)
+                    s += fold[g * S.tiles + tile];
+                const int row = r0 + x, col = cc0 + y;
+                int e = -1;
+                if (row < VP)
+                {
+                    if (row < mm && col < mm && col >= row)
+                        e = tri_index(row, col, mm);
+                }
+                else
+                {
+                    const int c = row - VP;
+                    if (c < nout && col < mm)
+                        e = S.mm * (S.mm + 1) / 2 + c * mm + col;
+                }
+                if (e >= 0)
+                    A.partial[((size_t)pl * A.entries + e) * LS_GRID + blockIdx.x] = s;
+            }
+        }
+}
+
+__global__ void k_ls_reduce(const double* partial, int entries, int planes, const double* omega, double* out)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= entries)
+        return;
+    double total = 0.0;
+    for (int p = 0; p < planes; p++)
+    {
+        const double* row = partial + ((size_t)p * entries + e) * LS_GRID;
+        double sum = 0.0;
+        for (int b = 0; b < LS_GRID; b++)
+            sum += row[b];
+        total += omega[p] * sum;
+    }
+    out[e] = total;
+}
+
+int normal_equations(nntc_b200_device* d, int k, const double* per_site, double* ms)
+{
+    const LsShape S = ls_shape(d->nin, d->nout);
+    const int mm = S.mm;
+    const int entries = mm * (mm + 1) / 2 + d->nout * mm;
+    if (!d->ls_partial)
+        NB_CUDA(cudaMalloc(&d->ls_partial, ((size_t)d->planes.size() * entries * LS_GRID + MAX_PLANES) *
+                                               sizeof(double)));
+    double* omega = d->ls_partial + (size_t)d->planes.size() * entries * LS_GRID;
+    NB_CUDA(cudaMemcpyAsync(omega, per_site, d->planes.size() * sizeof(double), cudaMemcpyHostToDevice, d->stream));
+    Planes P = planes_for(d, 0, [&](int) { return (size_t)0; });
+    P.kc = k;
+    NB_TRY(block_begin(d));
+    dim3 grid(LS_GRID, (unsigned)P.n);
+    const size_t shared = LS_THREADS * sizeof(double) + (size_t)(S.nv + S.nt) * TILE * LS_STRIDE * sizeof(float);
+    NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
+    k_ls_accumulate<<<grid, LS_THREADS, shared, d->stream>>>(P, S, LsArgs{ d->ls_partial, entries });
+    NB_LAUNCHED();
+    k_ls_reduce<<<grid_for((size_t)entries, 128), 128, 0, d->stream>>>(d->ls_partial, entries, P.n, omega,
+                                                                      d->reduction);
+    NB_LAUNCHED();
+    return block_end(d, ms);
+}
+
+// ---- the host solve (src/solve_decoder.cu:184-458) -----------------------------------------------------------------
+
+static bool gauss_jordan(std::vector<double>& g, int m, int nrhs)
+{
+    const int cols = m + nrhs;
+    for (int k = 0; k < m; k++)
+    {
+        int pivot = k;
+        double best = std::fabs(g[(size_t)k * cols + k]);
+        for (int i = k + 1; i < m; i++)
+        {
+            const double a = std::fabs(g[(size_t)i * cols + k]);
+            if (a > best)
+            {
+                best = a;
+                pivot = i;
+            }
+        }
+        if (best == 0.0)
+            return false;
+        if (pivot != k)
+            for (int j = 0; j < cols; j++)
+                std::swap(g[(size_t)k * cols + j], g[(size_t)pivot * cols + j]);
+        const double inv = 1.0 / g[(size_t)k * cols + k];
+        for (int j = 0; j < cols; j++)
+            g[(size_t)k * cols + j] *= inv;
+        for (int i = 0; i < m; i++)
+        {
+            if (i == k)
+                continue;
+            const double f = g[(size_t)i * cols + k];
+            if (f == 0.0)
+                continue;
+            for (int j = 0; j < cols; j++)
+                g[(size_t)i * cols + j] -= f * g[(size_t)k * cols + j];
+        }
+    }
+    return true;
+}
+
+static const double RIDGE_LADDER[] = { 1e-9, 1e-12, 0.0 };
+static const double LS_ACCEPT_RISE = 1e-12;
+static long long g_ridge_tally[4] = { 0, 0, 0, 0 };
+
+// The decoder from the normal equations in acc (the ladder, the acceptance test and the fallbacks). Returns the rung
+// taken (0..2), or 3 when every rung was refused.
+int decoder_from_normal_equations(nntc_b200_model& m, int k, const double* per_site, const std::vector<double>& acc)
+{
+    const int nin = m.nin, nout = m.nout, mm = nin + 1;
+    const int tri = mm * (mm + 1) / 2;
+    double trace = 0.0;
+    for (int i = 0; i < mm; i++)
+        trace += acc[(size_t)tri_index(i, i, mm)];
+    const double mean_diag = trace > 0.0 ? trace / mm : 1.0;
+
+    const bool had_previous = m.has_decoder != 0;
+    std::vector<double> x_prev((size_t)nout * mm, 0.0);
+    if (had_previous)
+        for (int c = 0; c < nout; c++)
+        {
+            for (int i = 0; i < nin; i++)
+                x_prev[(size_t)c * mm + i] = (double)m.dec_w[(size_t)c * nin + i];
+            x_prev[(size_t)c * mm + nin] = (double)m.dec_b[c];
+        }
+    double sum_cw = 0.0;
+    for (int c = 0; c < nout; c++)
+        sum_cw += (double)m.cw[c];
+    double den = 0.0;
+    for (int i = 0; i < m.nplanes; i++)
+        den += per_site[i] * (double)m.w0[i] * (double)m.h0[i] * (double)(1 + k);
+    const bool norm_ok = sum_cw * den > 0.0;
+    const double inv_norm = norm_ok ? 1.0 / (sum_cw * den) : 0.0;
+
+    auto qform = [&](const std::vector<double>& x, double& err) {
+        double q = 0.0, e = 0.0;
+        for (int c = 0; c < nout; c++)
+        {
+            double qc = 0.0, ec = 0.0;
+            for (int i = 0; i < mm; i++)
+            {
+                for (int j = 0; j < mm; j++)
+                {
+                    const double a = i <= j ? acc[(size_t)tri_index(i, j, mm)] : acc[(size_t)tri_index(j, i, mm)];
+                    qc += x[(size_t)c * mm + i] * a * x[(size_t)c * mm + j];
+                    ec += std::fabs(x[(size_t)c * mm + i]) * std::fabs(a) * std::fabs(x[(size_t)c * mm + j]);
+                }
+                qc -= 2.0 * x[(size_t)c * mm + i] * acc[(size_t)tri + (size_t)c * mm + i];
+                ec += 2.0 * std::fabs(x[(size_t)c * mm + i]) * std::fabs(acc[(size_t)tri + (size_t)c * mm + i]);
+            }
+            q += (double)m.cw[c] * qc;
+            e += (double)m.cw[c] * ec;
+        }
+        err = DBL_EPSILON * (double)mm * e * inv_norm;
+        return q;
+    };
+
+    double err_prev = 0.0;
+    const double q_prev = had_previous ? qform(x_prev, err_prev) : 0.0;
+    const int cols = mm + nout;
+    std::vector<double> g((size_t)mm * cols, 0.0);
+    std::vector<double> x_new((size_t)nout * mm, 0.0);
+    bool accepted = false;
+    int taken = 0;
+    for (int step = 0; step < 3 && !accepted; step++)
+    {
+        const double ridge = RIDGE_LADDER[step] * mean_diag;
+        std::fill(g.begin(), g.end(), 0.0);
+        for (int i = 0; i < mm; i++)
+        {
+            for (int j = i; j < mm; j++)
+            {
+                const double a = acc[(size_t)tri_index(i, j, mm)];
+                g[(size_t)i * cols + j] = a;
+                g[(size_t)j * cols + i] = a;
+            }
+            g[(size_t)i * cols + i] += ridge;
+            for (int c = 0; c < nout; c++)
+                g[(size_t)i * cols + mm + c] = acc[(size_t)tri + (size_t)c * mm + i];
+        }
+        if (!gauss_jordan(g, mm, nout))
+            continue;
+        bool finite = true;
+        for (int c = 0; c < nout; c++)
+            for (int i = 0; i < mm; i++)
+            {
+                const double v = (double)(float)g[(size_t)i * cols + mm + c];
+                x_new[(size_t)c * mm + i] = v;
+                finite = finite && std::isfinite(v);
+            }
+        if (!finite)
+            continue;
+        double err_cand = 0.0;
+        const double q_cand = qform(x_new, err_cand);
+        if (!had_previous || (norm_ok && (q_cand - q_prev) * inv_norm + err_prev + err_cand <= LS_ACCEPT_RISE))
+        {
+            accepted = true;
+            taken = step;
+        }
+    }
+    g_ridge_tally[accepted ? taken : 3]++;
+    if (accepted)
+    {
+        for (int c = 0; c < nout; c++)
+        {
+            for (int i = 0; i < nin; i++)
+                m.dec_w[(size_t)c * nin + i] = (float)x_new[(size_t)c * mm + i];
+            m.dec_b[c] = (float)x_new[(size_t)c * mm + nin];
+        }
+        m.has_decoder = 1;
+    }
+    else if (!had_previous)
+    {
+        for (int i = 0; i < nout * nin; i++)
+            m.dec_w[i] = 0.0f;
+        const double count = acc[(size_t)tri_index(nin, nin, mm)];
+        for (int c = 0; c < nout; c++)
+            m.dec_b[c] = count > 0.0 ? (float)(acc[(size_t)tri + (size_t)c * mm + nin] / count) : 0.0f;
+        m.has_decoder = 1;
+    }
+    return accepted ? taken : 3;
+}
+
+}   // namespace nb
+
+using namespace nb;
+
+extern "C"
+{
+
+int nntc_b200_solve_decoder(nntc_b200_device* d, nntc_b200_model* m, int k, const double* per_site, double* ms)
+{
+    double t = 0.0;
+    NB_TRY(normal_equations(d, k, per_site, &t));
+    const int mm = d->nin + 1;
+    std::vector<double> acc((size_t)(mm * (mm + 1) / 2 + d->nout * mm));
+    NB_TRY(download(d, acc.data(), d->reduction, acc.size() * sizeof(double)));
+    decoder_from_normal_equations(*m, k, per_site, acc);
+    NB_TRY(upload_decoder(d, m));
+    if (ms)
+        *ms = t;
+    return NNTC_B200_OK;
+}
+
+void nntc_b200_decoder_ridge_tally(long long out[4])
+{
+    for (int i = 0; i < 4; i++)
+        out[i] = g_ridge_tally[i];
+}
+
+}   // extern "C"

@@ -1,0 +1,341 @@
+// objective.cu: the objective E over every site of every plane, and the encoder's own 8-bit decode of a level.
+//
+// Follows src/objective.cu:53-279: E = sum_m w_m sum_sites sum_c cw_c (W phi + b - t)_c^2 with phi and the target
+// sampled in double at u = (px + 0.5 + dx) / w0 (src/objective.cu:97-118), plus the unweighted centre-site and
+// fractional-site sums per plane, normalised on the host (src/objective.cu:224-250).
+//
+// B200 shape: one thread per pixel handles that pixel's 1 + K sites, every plane of the chain in ONE launch (the
+// per-plane pixel ranges are padded to whole blocks, so a block belongs to one plane); the decoder sits in shared
+// memory as doubles; each block writes one partial per sum, and a second kernel adds a plane's partials in block
+// order. The dot products use DFMA: the per-site value differs from the reference's separately-rounded multiply-add
+// in the last bits only, and E is a measurement held to 1e-9 relative of the host twin (src/objective.cu:317-380).
+
+#include <cmath>
+#include <vector>
+
+#include "device.cuh"
+
+namespace nb
+{
+
+constexpr int OBJ_THREADS = 256;
+
+struct ObjArgs
+{
+    const float* weights;
+    const float* bias;
+    const float* cw;
+    double* partial;   // [3][total blocks]
+};
+
+__device__ __forceinline__ void obj_sample(const float* plane, int w, int h, int c, double u, double v, double* out)
+{
+    const double x = u * (double)w - 0.5, y = v * (double)h - 0.5;
+    const double xf = floor(x), yf = floor(y);
+    const double fx = x - xf, fy = y - yf;
+    const int x0 = clampi((int)xf, w), x1 = clampi((int)xf + 1, w);
+    const int y0 = clampi((int)yf, h), y1 = clampi((int)yf + 1, h);
+    const float* a = plane + ((size_t)y0 * w + x0) * c;
+    const float* b = plane + ((size_t)y0 * w + x1) * c;
+    const float* e = plane + ((size_t)y1 * w + x0) * c;
+    const float* f = plane + ((size_t)y1 * w + x1) * c;
+    const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy), w01 = (1.0 - fx) * fy, w11 = fx * fy;
+    for (int k = 0; k < c; k++)
+        out[k] = w00 * (double)__ldg(a + k) + w10 * (double)__ldg(b + k) + w01 * (double)__ldg(e + k) +
+                 w11 * (double)__ldg(f + k);
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0)
+        sh[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++)
+            s += sh[i];
+    return s;   // valid on thread 0
+}
+
+__global__ void __launch_bounds__(OBJ_THREADS) k_objective(Planes P, ObjArgs A)
+{
+    __shared__ double sw[MAX_NOUT * MAX_NIN];
+    __shared__ double sb[MAX_NOUT];
+    __shared__ double scw[MAX_NOUT];
+    __shared__ double red[32];
+    const int nin = P.nin, nout = P.nout, c0 = P.c0, c1 = P.c1, kc = P.kc;
+    for (int i = threadIdx.x; i < nout * nin; i += blockDim.x)
+        sw[i] = (double)A.weights[i];
+    for (int i = threadIdx.x; i < nout; i += blockDim.x)
+    {
+        sb[i] = (double)A.bias[i];
+        scw[i] = (double)A.cw[i];
+    }
+    __syncthreads();
+
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long local = base - P.start[pl] + threadIdx.x;
+    double weighted = 0.0, centre = 0.0, fractional = 0.0;
+    if (local < (long long)V.w0 * V.h0)
+    {
+        const int px = (int)(local % V.w0), py = (int)(local / V.w0);
+        for (int j = 0; j <= kc; j++)
+        {
+            float dx = 0.0f, dy = 0.0f;
+            if (j > 0)
+                subtexel(kc, j - 1, px, py, dx, dy);
+            const double u = ((double)px + 0.5 + (double)dx) / (double)V.w0;
+            const double v = ((double)py + 0.5 + (double)dy) / (double)V.h0;
+            double s[MAX_CH], c[MAX_CH], t[MAX_NOUT];
+            obj_sample(V.v1, V.w1, V.h1, c1, u, v, c);
+            if (j == 0)
+            {
+                for (int i = 0; i < c0; i++)
+                    s[i] = (double)V.v0[local * c0 + i];
+                for (int i = 0; i < nout; i++)
+                    t[i] = (double)__ldg(V.src + local * nout + i);
+            }
+            else
+            {
+                obj_sample(V.v0, V.w0, V.h0, c0, u, v, s);
+                obj_sample(V.src, V.w0, V.h0, nout, u, v, t);
+            }
+            double phi[MAX_NIN];
+            features(s, c0, c, c1, phi);
+            for (int r = 0; r < nout; r++)
+            {
+                double acc = sb[r];
+                const double* row = sw + r * nin;
+                for (int i = 0; i < nin; i++)
+                    acc = fma(row[i], phi[i], acc);
+                const double e = acc - t[r];
+                weighted = fma(scw[r] * e, e, weighted);
+                if (j == 0)
+                    centre = fma(e, e, centre);
+                else
+                    fractional = fma(e, e, fractional);
+            }
+        }
+    }
+    const double a = block_sum(weighted, red);
+    const double b = block_sum(centre, red);
+    const double c = block_sum(fractional, red);
+    if (threadIdx.x == 0)
+    {
+        const size_t nb = gridDim.x;
+        A.partial[blockIdx.x] = a;
+        A.partial[nb + blockIdx.x] = b;
+        A.partial[2 * nb + blockIdx.x] = c;
+    }
+}
+
+// One block per plane: the plane's block partials added in a fixed order (a strided pass, then a fixed tree).
+__global__ void k_objective_reduce(Planes P, const double* partial, int nblocks, double* out)
+{
+    __shared__ double red[32];
+    const int pl = blockIdx.x;
+    const long long b0 = P.start[pl] / OBJ_THREADS, b1 = P.start[pl + 1] / OBJ_THREADS;
+    for (int row = 0; row < 3; row++)
+    {
+        double s = 0.0;
+        for (long long b = b0 + threadIdx.x; b < b1; b += blockDim.x)
+            s += partial[(size_t)row * nblocks + b];
+        const double t = block_sum(s, red);
+        if (threadIdx.x == 0)
+            out[3 * pl + row] = t;
+        __syncthreads();
+    }
+}
+
+// The recon decode at texel centres: saturate, then lroundf(acc * 255) (src/objective.cu:53-75).
+__global__ void k_decode(const float* v0, const float* v1, int w0, int h0, int w1, int h1, int c0, int c1, int nin,
+                         int nout, const float* weights, const float* bias, uint8_t* out)
+{
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)w0 * h0)
+        return;
+    const int px = (int)(idx % (size_t)w0), py = (int)(idx / (size_t)w0);
+    float s[MAX_CH], c[MAX_CH], phi[MAX_NIN];
+    for (int i = 0; i < c0; i++)
+        s[i] = v0[idx * c0 + i];
+    const Tap t = tap_at(px, py, 0.0f, 0.0f, w0, h0, w1, h1);
+    blend<MAX_CH>(v1, w1, c1, t, c);
+    features(s, c0, c, c1, phi);
+    for (int r = 0; r < nout; r++)
+    {
+        float acc = bias[r];
+        const float* row = weights + (size_t)r * nin;
+        for (int i = 0; i < nin; i++)
+            acc += row[i] * phi[i];
+        acc = acc < 0.0f ? 0.0f : (acc > 1.0f ? 1.0f : acc);
+        out[idx * nout + r] = (uint8_t)lroundf(acc * 255.0f);
+    }
+}
+
+// The reported numbers from the three raw sums per plane (src/objective.cu:224-250).
+static void normalise(const nntc_b200_model& m, int k, const double* per_site, const std::vector<double>& acc,
+                      nntc_b200_objective* r)
+{
+    double sum_cw = 0.0;
+    for (int c = 0; c < m.nout; c++)
+        sum_cw += (double)m.cw[c];
+    double num = 0.0, den = 0.0;
+    for (int p = 0; p < m.nplanes; p++)
+    {
+        const double pixels = (double)m.w0[p] * (double)m.h0[p];
+        const double sites = pixels * (double)(1 + k);
+        r->e_plane[p] = acc[3 * p] / (sum_cw * sites);
+        r->centre_plane[p] = acc[3 * p + 1] / (pixels * (double)m.nout);
+        num += per_site[p] * acc[3 * p];
+        den += per_site[p] * sites;
+    }
+    r->e = den > 0.0 ? num / (sum_cw * den) : 0.0;
+    const double base = (double)m.w0[0] * (double)m.h0[0] * (double)m.nout;
+    r->centre_mse = acc[1] / base;
+    r->sampled_mse = k > 0 ? acc[2] / (base * (double)k) : 0.0;
+}
+
+static double g_objective_ms = 0.0;
+static long long g_objective_calls = 0;
+
+// The raw sums of every plane, three per plane, into host memory (acc has 3 nplanes entries).
+int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double* ms)
+{
+    Planes P = planes_for(d, 0, [&](int i) { return (size_t)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0; });
+    P.kc = k;
+    const int nblocks = (int)(P.start[P.n] / OBJ_THREADS);
+    // device_create sized obj_partial for this layout: 3 doubles per pixel block, then 3 sums per plane.
+    double* sums = d->obj_partial + (size_t)nblocks * 3;
+    ObjArgs A{ d->weights, d->bias, d->cw, d->obj_partial };
+    NB_TRY(block_begin(d));
+    k_objective<<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, A);
+    NB_LAUNCHED();
+    k_objective_reduce<<<P.n, 256, 0, d->stream>>>(P, d->obj_partial, nblocks, sums);
+    NB_LAUNCHED();
+    NB_TRY(block_end(d, ms));
+    acc.assign((size_t)3 * P.n, 0.0);
+    return download(d, acc.data(), sums, acc.size() * sizeof(double));
+}
+
+}   // namespace nb
+
+using namespace nb;
+
+extern "C"
+{
+
+int nntc_b200_objective_eval(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                             nntc_b200_objective* r)
+{
+    std::vector<double> acc;
+    double ms = 0.0;
+    NB_TRY(objective_sums(d, k, acc, &ms));
+    *r = nntc_b200_objective{};
+    normalise(*m, k, per_site, acc, r);
+    r->ms = ms;
+    g_objective_ms += ms;
+    g_objective_calls++;
+    return NNTC_B200_OK;
+}
+
+double nntc_b200_objective_total_ms(void)
+{
+    return g_objective_ms;
+}
+
+long long nntc_b200_objective_passes(void)
+{
+    return g_objective_calls;
+}
+
+int nntc_b200_decode_plane(nntc_b200_device* d, const nntc_b200_model* m, int plane, uint8_t* rgb8, size_t n)
+{
+    NB_TRY(check_plane(d, plane));
+    const DevPlane& p = d->planes[(size_t)plane];
+    const size_t px = (size_t)p.w0 * p.h0;
+    if (n < px * m->nout)
+    {
+        set_error(NNTC_B200_ERR_ARG, "decode buffer too small");
+        return NNTC_B200_ERR_ARG;
+    }
+    k_decode<<<grid_for(px, 256), 256, 0, d->stream>>>(p.v0, p.v1, p.w0, p.h0, p.w1, p.h1, d->c0, d->c1, d->nin,
+                                                      d->nout, d->weights, d->bias, d->rgb8);
+    NB_LAUNCHED();
+    return download(d, rgb8, d->rgb8, px * m->nout);
+}
+
+// The brute-force host twin (src/objective.cu:317-380): every plane downloaded and walked site by site in double.
+int nntc_b200_objective_check_host(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                                   nntc_b200_objective* r)
+{
+    const int c0 = m->c0, c1 = m->c1, nout = m->nout, nin = m->nin;
+    std::vector<double> acc((size_t)3 * m->nplanes, 0.0);
+    auto sample = [](const std::vector<float>& plane, int w, int h, int c, double u, double v, double* out) {
+        const double x = u * (double)w - 0.5, y = v * (double)h - 0.5;
+        const double xf = std::floor(x), yf = std::floor(y);
+        const double fx = x - xf, fy = y - yf;
+        const int x0 = clampi((int)xf, w), x1 = clampi((int)xf + 1, w);
+        const int y0 = clampi((int)yf, h), y1 = clampi((int)yf + 1, h);
+        for (int q = 0; q < c; q++)
+        {
+            const double a = plane[((size_t)y0 * w + x0) * c + q], b = plane[((size_t)y0 * w + x1) * c + q];
+            const double e = plane[((size_t)y1 * w + x0) * c + q], f = plane[((size_t)y1 * w + x1) * c + q];
+            out[q] = (1.0 - fx) * (1.0 - fy) * a + fx * (1.0 - fy) * b + (1.0 - fx) * fy * e + fx * fy * f;
+        }
+    };
+    for (int pl = 0; pl < m->nplanes; pl++)
+    {
+        const DevPlane& dp = d->planes[(size_t)pl];
+        std::vector<float> v0((size_t)dp.w0 * dp.h0 * c0), v1((size_t)dp.w1 * dp.h1 * c1),
+            src((size_t)dp.w0 * dp.h0 * nout);
+        NB_TRY(download(d, v0.data(), dp.v0, v0.size() * sizeof(float)));
+        NB_TRY(download(d, v1.data(), dp.v1, v1.size() * sizeof(float)));
+        NB_TRY(download(d, src.data(), dp.src, src.size() * sizeof(float)));
+        for (int py = 0; py < dp.h0; py++)
+            for (int px = 0; px < dp.w0; px++)
+                for (int j = 0; j <= k; j++)
+                {
+                    float dx = 0.0f, dy = 0.0f;
+                    if (j > 0)
+                        subtexel(k, j - 1, px, py, dx, dy);
+                    const double u = ((double)px + 0.5 + (double)dx) / (double)dp.w0;
+                    const double v = ((double)py + 0.5 + (double)dy) / (double)dp.h0;
+                    double s[MAX_CH], c[MAX_CH], t[MAX_NOUT], phi[MAX_NIN];
+                    sample(v1, dp.w1, dp.h1, c1, u, v, c);
+                    if (j == 0)
+                    {
+                        const size_t idx = (size_t)py * dp.w0 + px;
+                        for (int i = 0; i < c0; i++)
+                            s[i] = v0[idx * c0 + i];
+                        for (int i = 0; i < nout; i++)
+                            t[i] = src[idx * nout + i];
+                    }
+                    else
+                    {
+                        sample(v0, dp.w0, dp.h0, c0, u, v, s);
+                        sample(src, dp.w0, dp.h0, nout, u, v, t);
+                    }
+                    features(s, c0, c, c1, phi);
+                    for (int row = 0; row < nout; row++)
+                    {
+                        double y = (double)m->dec_b[row];
+                        for (int i = 0; i < nin; i++)
+                            y += (double)m->dec_w[(size_t)row * nin + i] * phi[i];
+                        const double e = y - t[row];
+                        acc[3 * pl] += (double)m->cw[row] * e * e;
+                        acc[3 * pl + (j == 0 ? 1 : 2)] += e * e;
+                    }
+                }
+    }
+    *r = nntc_b200_objective{};
+    normalise(*m, k, per_site, acc, r);
+    return NNTC_B200_OK;
+}
+
+}   // extern "C"

@@ -1,0 +1,781 @@
+// refine.cu: the BC4/BC5 pack of level 0 and its refinement by analysis by synthesis (src/refine_bc.cu).
+//
+// With level 1 and the decoder held, E is an exact quadratic in level 0's values; restricted to one 4x4 block with
+// every texel outside it held it is E_blk(d) = const + 2 A1.d + d^T A2 d (src/refine_bc.cu:15-45). Per block and
+// channel the endpoints move by a 2x2 least squares with its nine rounded candidates, then two Gauss-Seidel passes
+// of exact 8-way selector argmins; a step is taken only on a strict decrease weighed in the float arithmetic the
+// file decodes in (src/refine_bc.cu:47-95). Four colours over the block grid keep every block's neighbourhood frozen.
+//
+// B200 shape: ONE WARP PER 4x4 BLOCK, with the block's A2 (up to 64 x 64 doubles) in shared memory. Every value is
+// computed with the arithmetic of the reference's CPU transcription (src/cpu/cpu_refine_bc.cpp:134-400), including
+// its order of summation: each block sum is a SERIAL fold over the sixteen texels in increasing order, which a warp
+// reproduces exactly by shuffling the sixteen per-lane terms to every lane and folding them in texel order. The
+// selector argmin evaluates its eight candidates on eight lanes and scans them in candidate order. Given the same
+// stencil, gradient and planes the endpoints and selectors are therefore the same bytes as the reference's.
+//
+// The seed pack (src/export.cpp:294-328 over shared/bc_pack.h:95-188) runs here on the device as well: one thread
+// per block-channel, integer arithmetic and the same float palette distances.
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "device.cuh"
+
+namespace nb
+{
+
+constexpr int REFINE_WARPS = 2;   // 4x4 blocks per CTA
+
+__host__ __device__ __forceinline__ double bc4_weight8(int sel)
+{
+    return sel == 0 ? 1.0 : (sel == 1 ? 0.0 : (double)(8 - sel) / 7.0);
+}
+
+__host__ __device__ __forceinline__ float bc4_entry(int r0, int r1, int sel)
+{
+    if (sel == 0)
+        return (float)r0;
+    if (sel == 1)
+        return (float)r1;
+    return (float)((8 - sel) * r0 + (sel - 1) * r1) / 7.0f;
+}
+
+__host__ __device__ __forceinline__ float bc0_value(float lo, float hi, float byte)
+{
+    const double frac = (double)byte / 255.0;
+    const double span = (double)hi - (double)lo;
+#ifdef __CUDA_ARCH__
+    return (float)__dadd_rn((double)lo, __dmul_rn(frac, span));
+#else
+    return (float)((double)lo + frac * span);
+#endif
+}
+
+__host__ __device__ __forceinline__ uint8_t bc0_index(float byte)
+{
+    return (uint8_t)(byte < 0.0f ? 0 : (byte > 255.0f ? 255 : (int)(byte + 0.5f)));
+}
+
+// The palette as a decoder evaluates it (shared/bc_pack.h:62-77), both modes.
+__host__ __device__ __forceinline__ void bc4_palette(int r0, int r1, float p[8])
+{
+    p[0] = (float)r0;
+    p[1] = (float)r1;
+    if (r0 > r1)
+    {
+        for (int i = 2; i < 8; i++)
+            p[i] = (float)((8 - i) * r0 + (i - 1) * r1) / 7.0f;
+    }
+    else
+    {
+        for (int i = 2; i < 6; i++)
+            p[i] = (float)((6 - i) * r0 + (i - 1) * r1) / 5.0f;
+        p[6] = 0.0f;
+        p[7] = 255.0f;
+    }
+}
+
+// One block of one channel (shared/bc_pack.h:95-166): sixteen stored bytes at `bits` bits, edge-clamped by the
+// caller, to endpoints and selectors.
+__host__ __device__ inline void bc4_seed_block(const uint8_t v[16], int bits, int& r0, int& r1, uint8_t sel[16])
+{
+    if (bits <= 3)
+    {
+        if (bits == 3)
+        {
+            r0 = 255;
+            r1 = 0;
+            for (int t = 0; t < 16; t++)
+            {
+                const int k = v[t] >> 5;
+                sel[t] = (uint8_t)(k == 7 ? 0 : (k == 0 ? 1 : 8 - k));
+            }
+        }
+        else if (bits == 2)
+        {
+            r0 = 85;
+            r1 = 170;
+            for (int t = 0; t < 16; t++)
+            {
+                const int k = v[t] >> 6;
+                sel[t] = (uint8_t)(k == 0 ? 6 : (k == 1 ? 0 : (k == 2 ? 1 : 7)));
+            }
+        }
+        else
+        {
+            r0 = 0;
+            r1 = 255;
+            for (int t = 0; t < 16; t++)
+                sel[t] = (uint8_t)((v[t] >> 7) ? 7 : 6);
+        }
+        return;
+    }
+    const int levels = (1 << bits) - 1;
+    int kmin = levels, kmax = 0;
+    for (int t = 0; t < 16; t++)
+    {
+        const int k = v[t] >> (8 - bits);
+        kmin = k < kmin ? k : kmin;
+        kmax = k > kmax ? k : kmax;
+    }
+    r0 = (int)llround(kmax * 255.0 / levels);
+    r1 = (int)llround(kmin * 255.0 / levels);
+    if (r0 == r1)
+    {
+        for (int t = 0; t < 16; t++)
+            sel[t] = 0;
+        return;
+    }
+    float p[8];
+    bc4_palette(r0, r1, p);
+    for (int t = 0; t < 16; t++)
+    {
+        const float target = (float)(v[t] >> (8 - bits)) * 255.0f / (float)levels;
+        int best = 0;
+        float best_d = 1e30f;
+        for (int i = 0; i < 8; i++)
+        {
+            const float d = fabsf(p[i] - target);
+            if (d < best_d)
+            {
+                best_d = d;
+                best = i;
+            }
+        }
+        sel[t] = (uint8_t)best;
+    }
+}
+
+struct BcPlane
+{
+    int w0, h0, bx;
+    uint8_t* ep;
+    uint8_t* sel;
+    const uint8_t* k0src;   // the indices the seed pack reads
+    float* v0;
+    uint8_t* k0;
+    double* delta;
+    const float* prev;
+    const double* stencil;  // SoA level-0 stencil
+    const double* grad;
+};
+
+struct BcPlanes
+{
+    int n, c0;
+    int bits[MAX_CH];
+    long long start[MAX_PLANES + 1];
+    BcPlane p[MAX_PLANES];
+};
+
+__device__ __forceinline__ int bc_plane_of(const BcPlanes& P, long long i)
+{
+    int lo = 0;
+    while (lo + 1 < P.n && P.start[lo + 1] <= i)
+        lo++;
+    return lo;
+}
+
+// One thread per block-channel: the stb_dxt-style seed (src/export.cpp:294-328).
+__global__ void k_bc_seed(BcPlanes P)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.start[P.n])
+        return;
+    const int pl = bc_plane_of(P, i);
+    const BcPlane& B = P.p[pl];
+    const long long local = i - P.start[pl];
+    const int c0 = P.c0;
+    const long long blk = local / c0;
+    const int c = (int)(local % c0);
+    if (blk >= (long long)B.bx * ((B.h0 + 3) / 4))
+        return;
+    const int gx = (int)(blk % B.bx), gy = (int)(blk / B.bx);
+    const int bits = P.bits[c];
+    uint8_t v[16];
+    for (int t = 0; t < 16; t++)
+    {
+        const int px = min(B.w0 - 1, gx * 4 + t % 4), py = min(B.h0 - 1, gy * 4 + t / 4);
+        v[t] = (uint8_t)rep_index((int)B.k0src[((size_t)py * B.w0 + px) * c0 + c], bits);
+    }
+    int r0, r1;
+    uint8_t sel[16];
+    bc4_seed_block(v, bits, r0, r1, sel);
+    const size_t slot = (size_t)blk * c0 + c;
+    B.ep[slot * 2] = (uint8_t)r0;
+    B.ep[slot * 2 + 1] = (uint8_t)r1;
+    for (int t = 0; t < 16; t++)
+        B.sel[slot * 16 + t] = sel[t];
+}
+
+// Endpoints and selectors to the plane, its indices and the correction (src/refine_bc.cu:155-174).
+__global__ void k_bc_decode(BcPlanes P, const float* lo0, const float* hi0)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.start[P.n])
+        return;
+    const int pl = bc_plane_of(P, i);
+    const BcPlane& B = P.p[pl];
+    const long long ti = i - P.start[pl];
+    if (ti >= (long long)B.w0 * B.h0)
+        return;
+    const int px = (int)(ti % B.w0), py = (int)(ti / B.w0);
+    const size_t gi = (size_t)(py / 4) * B.bx + (px / 4);
+    const int t = (py % 4) * 4 + (px % 4);
+    const int c0 = P.c0;
+    for (int c = 0; c < c0; c++)
+    {
+        const size_t b = gi * c0 + c;
+        const float byte = bc4_entry(B.ep[b * 2], B.ep[b * 2 + 1], B.sel[b * 16 + t]);
+        const float value = bc0_value(lo0[c], hi0[c], byte);
+        const size_t idx = (size_t)ti * c0 + c;
+        B.v0[idx] = value;
+        B.k0[idx] = bc0_index(byte);
+        B.delta[idx] = (double)value - (double)B.prev[idx];
+    }
+}
+
+// The sixteen lanes' terms folded serially in texel order, the same on every lane.
+__device__ __forceinline__ double fold16(double v)
+{
+    double s = 0.0;
+    for (int t = 0; t < 16; t++)
+        s += __shfl_sync(0xffffffffu, v, t);
+    return s;
+}
+
+struct RefineArgs
+{
+    const float* lo0;
+    const float* hi0;
+    int cx, cy;
+    double* stats;   // [plane][2]
+};
+
+// One warp per 4x4 block of the colour; the block of every plane of the chain in one launch (start[] counts blocks
+// of the colour per plane).
+__global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, RefineArgs R)
+{
+    extern __shared__ double smem[];
+    const int c0 = P.c0, n = 16 * c0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t per_warp = (size_t)n * n + 3 * (size_t)n + 16 + 16;
+    double* a2 = smem + warp * per_warp;
+    double* a1 = a2 + n * n;
+    double* dv = a1 + n;
+    double* uv = dv + n;
+    double* dlt = uv + n;
+    int* s_ep = (int*)(dlt + 16);            // 8 ints
+    unsigned char* s_sel = (unsigned char*)(s_ep + 8);   // 64 bytes (fits in the last 16 doubles with s_ep)
+
+    const long long bi = (long long)blockIdx.x * REFINE_WARPS + warp;
+    if (bi >= P.start[P.n])
+        return;
+    const int pl = bc_plane_of(P, bi);
+    const BcPlane& B = P.p[pl];
+    const long long local = bi - P.start[pl];
+    const int by = (B.h0 + 3) / 4;
+    const int cbx = (B.bx - R.cx + 1) / 2, cby = (by - R.cy + 1) / 2;
+    if (local >= (long long)cbx * cby)
+        return;
+    const int gx = R.cx + 2 * (int)(local % cbx);
+    const int gy = R.cy + 2 * (int)(local / cbx);
+    const int w0 = B.w0, h0 = B.h0;
+    const size_t T = (size_t)w0 * h0;
+    const int cc = c0 * c0;
+
+    for (int i = lane; i < n * n; i += 32)
+        a2[i] = 0.0;
+    for (int i = lane; i < n; i += 32)
+    {
+        a1[i] = 0.0;
+        dv[i] = 0.0;
+        uv[i] = 0.0;
+    }
+    __syncwarp();
+
+    // The block's quadratic, one lane per texel (src/cpu/cpu_refine_bc.cpp:152-205). Every A2 entry receives exactly
+    // one contribution, so the parallel writes need no order.
+    if (lane < 16)
+    {
+        const int tid = lane;
+        const int px = gx * 4 + (tid & 3), py = gy * 4 + (tid >> 2);
+        if (px < w0 && py < h0)
+        {
+            const size_t ti = (size_t)py * w0 + px;
+            double acc[MAX_CH];
+            for (int i = 0; i < c0; i++)
+                acc[i] = B.grad[ti * c0 + i];
+            for (int slot = 0; slot < SLOTS; slot++)
+            {
+                int dx, dy;
+                slot_offset(slot, dx, dy);
+                const int fx = px + dx, fy = py + dy;
+                if (fx >= 0 && fx < w0 && fy >= 0 && fy < h0)
+                {
+                    const int lx = fx - gx * 4, ly = fy - gy * 4;
+                    if (lx >= 0 && lx < 4 && ly >= 0 && ly < 4)
+                    {
+                        const int ft = ly * 4 + lx;
+                        for (int i = 0; i < c0; i++)
+                            for (int j = 0; j < c0; j++)
+                            {
+                                const double e = B.stencil[(size_t)(slot * cc + i * c0 + j) * T + ti];
+                                a2[(size_t)(tid * c0 + i) * n + (ft * c0 + j)] += e;
+                                if (slot != 0)
+                                    a2[(size_t)(ft * c0 + j) * n + (tid * c0 + i)] += e;
+                            }
+                    }
+                    else
+                    {
+                        const double* xn = B.delta + ((size_t)fy * w0 + fx) * c0;
+                        for (int i = 0; i < c0; i++)
+                            for (int j = 0; j < c0; j++)
+                                acc[i] += B.stencil[(size_t)(slot * cc + i * c0 + j) * T + ti] * xn[j];
+                    }
+                }
+                if (slot == 0)
+                    continue;
+                const int ax = px - dx, ay = py - dy;
+                const int lx = ax - gx * 4, ly = ay - gy * 4;
+                if (ax < 0 || ax >= w0 || ay < 0 || ay >= h0 || (lx >= 0 && lx < 4 && ly >= 0 && ly < 4))
+                    continue;
+                const size_t nt = (size_t)ay * w0 + ax;
+                const double* xn = B.delta + nt * c0;
+                for (int i = 0; i < c0; i++)
+                    for (int j = 0; j < c0; j++)
+                        acc[i] += B.stencil[(size_t)(slot * cc + j * c0 + i) * T + nt] * xn[j];
+            }
+            for (int i = 0; i < c0; i++)
+            {
+                a1[tid * c0 + i] = acc[i];
+                dv[tid * c0 + i] = (double)B.v0[ti * c0 + i] - (double)B.prev[ti * c0 + i];
+            }
+        }
+    }
+    __syncwarp();
+    for (int r = lane; r < n; r += 32)
+    {
+        double s = 0.0;
+        for (int j = 0; j < n; j++)
+            s += a2[(size_t)r * n + j] * dv[j];
+        uv[r] = s;
+    }
+    const size_t gi = (size_t)gy * B.bx + gx;
+    if (lane < c0)
+    {
+        s_ep[2 * lane] = B.ep[(gi * c0 + lane) * 2];
+        s_ep[2 * lane + 1] = B.ep[(gi * c0 + lane) * 2 + 1];
+    }
+    for (int i = lane; i < n; i += 32)
+        s_sel[i] = B.sel[gi * c0 * 16 + i];
+    __syncwarp();
+
+    double taken = 0.0;
+    // ---- (i) the endpoints of each channel (src/cpu/cpu_refine_bc.cpp:222-312)
+    for (int c = 0; c < c0; c++)
+    {
+        const double step = ((double)R.hi0[c] - (double)R.lo0[c]) / 255.0;
+        double tbp = 0.0, tbq = 0.0, tpap = 0.0, tpaq = 0.0, tqaq = 0.0;
+        if (lane < 16)
+        {
+            const int idx = lane * c0 + c;
+            const double a = bc4_weight8(s_sel[c * 16 + lane]);
+            const double p = step * a;
+            const double q = step * (1.0 - a);
+            const double b = a1[idx] + uv[idx];
+            double ap = 0.0, aq = 0.0;
+            for (int j = 0; j < 16; j++)
+            {
+                const double e = a2[(size_t)idx * n + (j * c0 + c)];
+                const double aj = bc4_weight8(s_sel[c * 16 + j]);
+                ap += e * step * aj;
+                aq += e * step * (1.0 - aj);
+            }
+            tbp = b * p;
+            tbq = b * q;
+            tpap = p * ap;
+            tpaq = p * aq;
+            tqaq = q * aq;
+        }
+        const double bp = fold16(tbp), bq = fold16(tbq), pap = fold16(tpap), paq = fold16(tpaq),
+                     qaq = fold16(tqaq);
+        const int r0 = s_ep[2 * c], r1 = s_ep[2 * c + 1];
+        const double det = pap * qaq - paq * paq;
+        double d0 = 0.0, d1 = 0.0;
+        if (det > 1e-12 * pap * qaq)
+        {
+            d0 = (paq * bq - qaq * bp) / det;
+            d1 = (paq * bp - pap * bq) / det;
+        }
+        const double v0r = (double)r0 + d0, v1r = (double)r1 + d1;
+        const int c0r = (int)floor(v0r + 0.5), c1r = (int)floor(v1r + 0.5);
+        double best = 0.0;
+        int best0 = r0, best1 = r1;
+        for (int e0 = -1; e0 <= 1; e0++)
+            for (int e1 = -1; e1 <= 1; e1++)
+            {
+                const int a0 = c0r + e0 < 0 ? 0 : (c0r + e0 > 255 ? 255 : c0r + e0);
+                const int a1i = c1r + e1 < 0 ? 0 : (c1r + e1 > 255 ? 255 : c1r + e1);
+                if (a0 <= a1i)
+                    continue;
+                const double f0 = (double)(a0 - r0), f1 = (double)(a1i - r1);
+                const double de = 2.0 * (bp * f0 + bq * f1) + pap * f0 * f0 + 2.0 * paq * f0 * f1 + qaq * f1 * f1;
+                if (de < best)
+                {
+                    best = de;
+                    best0 = a0;
+                    best1 = a1i;
+                }
+            }
+        if (best0 == r0 && best1 == r1)
+            continue;
+        if (lane < 16)
+        {
+            const float now = bc0_value(R.lo0[c], R.hi0[c], bc4_entry(r0, r1, s_sel[c * 16 + lane]));
+            const float next = bc0_value(R.lo0[c], R.hi0[c], bc4_entry(best0, best1, s_sel[c * 16 + lane]));
+            dlt[lane] = (double)next - (double)now;
+        }
+        __syncwarp();
+        double term = 0.0;
+        if (lane < 16)
+        {
+            const int idx = lane * c0 + c;
+            double quad = 0.0;
+            for (int j = 0; j < 16; j++)
+                quad += a2[(size_t)idx * n + (j * c0 + c)] * dlt[j];
+            term = dlt[lane] * (2.0 * (a1[idx] + uv[idx]) + quad);
+        }
+        const double exact = fold16(term);
+        if (exact < 0.0)
+        {
+            for (int r = lane; r < n; r += 32)
+            {
+                double add = 0.0;
+                for (int j = 0; j < 16; j++)
+                    add += a2[(size_t)r * n + (j * c0 + c)] * dlt[j];
+                uv[r] += add;
+            }
+            if (lane < 16)
+                dv[lane * c0 + c] += dlt[lane];
+            if (lane == 0)
+            {
+                s_ep[2 * c] = best0;
+                s_ep[2 * c + 1] = best1;
+            }
+            taken += exact;
+        }
+        __syncwarp();
+    }
+
+    // ---- (ii) the selectors: two Gauss-Seidel passes of exact 8-way argmins (src/cpu/cpu_refine_bc.cpp:314-345)
+    for (int pass = 0; pass < 2; pass++)
+        for (int c = 0; c < c0; c++)
+        {
+            const int r0 = s_ep[2 * c], r1 = s_ep[2 * c + 1];
+            const float lo = R.lo0[c], hi = R.hi0[c];
+            // the eight decoded values of this channel's palette, one per lane 0..7
+            const double cand = lane < 8 ? (double)bc0_value(lo, hi, bc4_entry(r0, r1, lane)) : 0.0;
+            for (int t = 0; t < 16; t++)
+            {
+                const int i = t * c0 + c;
+                const double b = a1[i] + uv[i], a = a2[(size_t)i * n + i];
+                const int cur = s_sel[c * 16 + t];
+                const double now = __shfl_sync(0xffffffffu, cand, cur);
+                const double d = cand - now;
+                const double de = 2.0 * b * d + a * d * d;
+                double best = 0.0, move = 0.0;
+                int which = cur;
+                for (int kk = 0; kk < 8; kk++)
+                {
+                    const double dk = __shfl_sync(0xffffffffu, de, kk);
+                    if (dk < best)
+                    {
+                        best = dk;
+                        move = __shfl_sync(0xffffffffu, d, kk);
+                        which = kk;
+                    }
+                }
+                // move and which are uniform: every lane ran the same scan over the same shuffled values
+                if (best < 0.0)
+                {
+                    for (int r = lane; r < n; r += 32)
+                        uv[r] += a2[(size_t)r * n + i] * move;
+                    if (lane == 0)
+                    {
+                        s_sel[c * 16 + t] = (unsigned char)which;
+                        dv[i] += move;
+                    }
+                    taken += best;
+                }
+                __syncwarp();
+            }
+        }
+
+    // ---- what the block leaves behind
+    if (lane < c0)
+    {
+        B.ep[(gi * c0 + lane) * 2] = (uint8_t)s_ep[2 * lane];
+        B.ep[(gi * c0 + lane) * 2 + 1] = (uint8_t)s_ep[2 * lane + 1];
+    }
+    for (int i = lane; i < n; i += 32)
+        B.sel[gi * c0 * 16 + i] = s_sel[i];
+    if (lane < 16)
+    {
+        const int px = gx * 4 + (lane & 3), py = gy * 4 + (lane >> 2);
+        if (px < w0 && py < h0)
+        {
+            const size_t ti = (size_t)py * w0 + px;
+            for (int c = 0; c < c0; c++)
+            {
+                const float byte = bc4_entry(s_ep[2 * c], s_ep[2 * c + 1], s_sel[c * 16 + lane]);
+                const float value = bc0_value(R.lo0[c], R.hi0[c], byte);
+                const size_t idx = ti * c0 + c;
+                B.v0[idx] = value;
+                B.k0[idx] = bc0_index(byte);
+                B.delta[idx] = (double)value - (double)B.prev[idx];
+            }
+        }
+    }
+    if (lane == 0 && taken < 0.0)
+    {
+        atomicAdd(R.stats + 2 * pl, taken);
+        atomicAdd(R.stats + 2 * pl + 1, 1.0);
+    }
+}
+
+template <class F>
+static BcPlanes bc_planes(nntc_b200_device* d, F items)
+{
+    BcPlanes P{};
+    P.n = (int)d->planes.size();
+    P.c0 = d->c0;
+    for (int c = 0; c < MAX_CH; c++)
+        P.bits[c] = d->m.bits0[c];
+    long long at = 0;
+    for (int i = 0; i < P.n; i++)
+    {
+        DevPlane& s = d->planes[(size_t)i];
+        BcPlane& b = P.p[i];
+        b.w0 = s.w0;
+        b.h0 = s.h0;
+        b.bx = (s.w0 + 3) / 4;
+        b.ep = s.bc_ep;
+        b.sel = s.bc_sel;
+        b.k0src = s.k0;
+        b.v0 = s.v0;
+        b.k0 = s.k0;
+        b.delta = s.work[1].x;
+        b.prev = s.work[1].prev;
+        b.stencil = s.work[1].stencil;
+        b.grad = s.work[1].grad;
+        P.start[i] = at;
+        at += (long long)items(i);
+    }
+    P.start[P.n] = at;
+    return P;
+}
+
+int assemble_for_refine(nntc_b200_device* d, const nntc_b200_model* m, int k, double* ms);
+
+int bc_decode_all(nntc_b200_device* d)
+{
+    BcPlanes P = bc_planes(d, [&](int i) { return (size_t)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0; });
+    k_bc_decode<<<grid_for((size_t)P.start[P.n], 256), 256, 0, d->stream>>>(P, d->lo0, d->hi0);
+    NB_LAUNCHED();
+    return NNTC_B200_OK;
+}
+
+int bc_prepare(nntc_b200_device* d, const nntc_b200_model* m, int k, int seed, const uint8_t* const* k0_host,
+               double* ms)
+{
+    if (!d->l0_bc8)
+    {
+        set_error(NNTC_B200_ERR_STATE, "the BC refinement runs only under --l0 bc8");
+        return NNTC_B200_ERR_STATE;
+    }
+    double t0 = 0.0, t1 = 0.0;
+    NB_TRY(assemble_for_refine(d, m, k, &t0));
+    if (seed)
+    {
+        // The seed pack reads the model's index mirror when the caller has one, else the device's own indices.
+        for (int i = 0; i < (int)d->planes.size(); i++)
+        {
+            DevPlane& p = d->planes[(size_t)i];
+            BcPlanes P = bc_planes(d, [&](int j) { return j == i ? p.blocks() * d->c0 : (size_t)0; });
+            if (k0_host && k0_host[i])
+            {
+                NB_TRY(upload(d, d->scratch8, k0_host[i], (size_t)p.w0 * p.h0 * d->c0));
+                P.p[i].k0src = d->scratch8;
+            }
+            k_bc_seed<<<grid_for((size_t)P.start[P.n], 128), 128, 0, d->stream>>>(P);
+            NB_LAUNCHED();
+        }
+    }
+    NB_TRY(block_begin(d));
+    NB_TRY(bc_decode_all(d));
+    NB_TRY(block_end(d, &t1));
+    if (ms)
+        *ms = t0 + t1;
+    return NNTC_B200_OK;
+}
+
+int bc_refine_passes(nntc_b200_device* d, const nntc_b200_model* m, int passes, nntc_b200_bc_report* rep, double* ms)
+{
+    (void)m;
+    double total = 0.0;
+    const int n = 16 * d->c0;
+    const size_t per_warp = (size_t)n * n + 3 * (size_t)n + 32;
+    const size_t shared = per_warp * REFINE_WARPS * sizeof(double);
+    NB_CUDA(cudaFuncSetAttribute(k_bc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
+    for (int pass = 0; pass < passes; pass++)
+    {
+        NB_CUDA(cudaMemsetAsync(d->bc_stats, 0, (size_t)MAX_PLANES * 2 * sizeof(double), d->stream));
+        NB_TRY(block_begin(d));
+        for (int colour = 0; colour < 4; colour++)
+        {
+            const int cx = colour & 1, cy = colour >> 1;
+            BcPlanes P = bc_planes(d, [&](int i) {
+                const DevPlane& p = d->planes[(size_t)i];
+                const int bx = (p.w0 + 3) / 4, by = (p.h0 + 3) / 4;
+                return (size_t)((bx - cx + 1) / 2) * (size_t)((by - cy + 1) / 2);
+            });
+            if (P.start[P.n] == 0)
+                continue;
+            RefineArgs R{ d->lo0, d->hi0, cx, cy, d->bc_stats };
+            const int grid = grid_for((size_t)P.start[P.n], REFINE_WARPS);
+            k_bc_refine<<<grid, 32 * REFINE_WARPS, shared, d->stream>>>(P, R);
+            NB_LAUNCHED();
+        }
+        double t = 0.0;
+        NB_TRY(block_end(d, &t));
+        total += t;
+        std::vector<double> stats((size_t)MAX_PLANES * 2);
+        NB_TRY(download(d, stats.data(), d->bc_stats, stats.size() * sizeof(double)));
+        nntc_b200_bc_report r{};
+        r.pass = pass + 1;
+        r.ms = t;
+        for (int i = 0; i < (int)d->planes.size(); i++)
+        {
+            r.delta_e += stats[(size_t)2 * i];
+            r.improved += (long long)stats[(size_t)2 * i + 1];
+            r.blocks += (long long)d->planes[(size_t)i].blocks();
+        }
+        if (rep)
+            rep[pass] = r;
+    }
+    if (ms)
+        *ms = total;
+    return NNTC_B200_OK;
+}
+
+}   // namespace nb
+
+using namespace nb;
+
+extern "C"
+{
+
+int nntc_b200_bc_pack_prepare(nntc_b200_device* d, const nntc_b200_model* m, int k, int seed,
+                              const uint8_t* const* k0_host, double* ms)
+{
+    return bc_prepare(d, m, k, seed, k0_host, ms);
+}
+
+int nntc_b200_bc_refine(nntc_b200_device* d, const nntc_b200_model* m, int passes, nntc_b200_bc_report* rep,
+                        double* ms)
+{
+    if (!d->l0_bc8)
+    {
+        set_error(NNTC_B200_ERR_STATE, "the BC refinement runs only under --l0 bc8");
+        return NNTC_B200_ERR_STATE;
+    }
+    return bc_refine_passes(d, m, passes, rep, ms);
+}
+
+int nntc_b200_bc_state_save(nntc_b200_device* d, const nntc_b200_model* m, uint8_t* const* ep, uint8_t* const* sel)
+{
+    (void)m;
+    for (size_t i = 0; i < d->planes.size(); i++)
+    {
+        const DevPlane& p = d->planes[i];
+        if (ep && ep[i])
+            NB_TRY(download(d, ep[i], p.bc_ep, p.blocks() * d->c0 * 2));
+        if (sel && sel[i])
+            NB_TRY(download(d, sel[i], p.bc_sel, p.blocks() * d->c0 * 16));
+    }
+    return NNTC_B200_OK;
+}
+
+int nntc_b200_bc_state_restore(nntc_b200_device* d, const nntc_b200_model* m, const uint8_t* const* ep,
+                               const uint8_t* const* sel)
+{
+    (void)m;
+    for (size_t i = 0; i < d->planes.size(); i++)
+    {
+        const DevPlane& p = d->planes[i];
+        if (ep && ep[i])
+            NB_TRY(upload(d, p.bc_ep, ep[i], p.blocks() * d->c0 * 2));
+        if (sel && sel[i])
+            NB_TRY(upload(d, p.bc_sel, sel[i], p.blocks() * d->c0 * 16));
+    }
+    return NNTC_B200_OK;
+}
+
+// The .dds bytes of one plane from endpoints and selectors, and the pack error against k0's exact index values
+// (src/export.cpp:262-279, 333-370; shared/bc_pack.h:79-85, 169-176). Host code: a few bytes per block.
+int nntc_b200_bc_pack_blocks(const nntc_b200_model* m, int plane, const uint8_t* ep, const uint8_t* sel,
+                             const uint8_t* k0, uint8_t* const* files, double* se, size_t* n)
+{
+    if (plane < 0 || plane >= m->nplanes)
+    {
+        set_error(NNTC_B200_ERR_ARG, "plane outside the model");
+        return NNTC_B200_ERR_ARG;
+    }
+    const int w0 = m->w0[plane], h0 = m->h0[plane], c0 = m->c0;
+    const int bx = (w0 + 3) / 4, by = (h0 + 3) / 4;
+    const int nfiles = c0 <= 2 ? 1 : 2;
+    for (int f = 0; f < nfiles; f++)
+    {
+        const int nc = f == 0 ? (c0 == 1 ? 1 : 2) : c0 - 2, bpb = nc == 1 ? 8 : 16;
+        for (int c = 0; c < nc; c++)
+        {
+            const int channel = 2 * f + c;
+            for (size_t b = 0; b < (size_t)bx * by; b++)
+            {
+                uint8_t* blk = files[f] + b * bpb + (size_t)c * 8;
+                const size_t slot = b * c0 + channel;
+                blk[0] = ep[slot * 2];
+                blk[1] = ep[slot * 2 + 1];
+                uint64_t bits = 0;
+                for (int t = 0; t < 16; t++)
+                    bits |= (uint64_t)(sel[slot * 16 + t] & 7) << (3 * t);
+                for (int i = 0; i < 6; i++)
+                    blk[2 + i] = (uint8_t)(bits >> (8 * i));
+            }
+            if (!k0)
+                continue;
+            for (int y = 0; y < h0; y++)
+                for (int x = 0; x < w0; x++)
+                {
+                    const uint8_t* blk = files[f] + ((size_t)(y / 4) * bx + x / 4) * bpb + (size_t)c * 8;
+                    float p[8];
+                    bc4_palette(blk[0], blk[1], p);
+                    uint64_t bits = 0;
+                    for (int i = 0; i < 6; i++)
+                        bits |= (uint64_t)blk[2 + i] << (8 * i);
+                    const float decoded = p[(bits >> (3 * ((y % 4) * 4 + x % 4))) & 7];
+                    const int b8 = m->l0_bc8 ? 8 : m->bits0[channel];
+                    const int kk = k0[((size_t)y * w0 + x) * c0 + channel];
+                    const double exact = b8 >= 8 ? (double)kk : (double)kk * 255.0 / (double)((1 << b8) - 1);
+                    const double e = (double)decoded - exact;
+                    *se += e * e;
+                    (*n)++;
+                }
+        }
+    }
+    return NNTC_B200_OK;
+}
+
+}   // extern "C"
