@@ -139,8 +139,12 @@ typedef struct nntc_b200_device nntc_b200_device;
 
 /* The message of the last failed call on this thread; "" when none failed. */
 const char* nntc_b200_last_error(void);
-/* 1 when this library was built for the device it finds (sm_100a kernels), else 0. */
+/* The ABI version of this header (1). */
 int nntc_b200_version(void);
+/* sizeof of the ABI's structs, in declaration order (model, device_info, plane_report, level0_report, objective,
+ * init1_report, init0_report, bc_report, encode_args, encode_result), so a foreign binding can check its mirror.
+ * Touches no device. Returns the count written (at most n). */
+int nntc_b200_abi_sizes(size_t* out, int n);
 
 /* ---- lifecycle: src/init.cu:76-382 (device_select, device_create, device_destroy, device_memory) ---- */
 int nntc_b200_device_select(int index, nntc_b200_device_info* info);           /* returns 1 if usable */
@@ -224,6 +228,45 @@ int nntc_b200_bc_state_restore(nntc_b200_device* d, const nntc_b200_model* m, co
  * blocks * (nc == 1 ? 8 : 16) bytes for file f (one file for 1-2 channels, two for 3-4). */
 int nntc_b200_bc_pack_blocks(const nntc_b200_model* m, int plane, const uint8_t* ep, const uint8_t* sel,
                              const uint8_t* k0, uint8_t* const* files, double* se, size_t* n);
+
+/* ---- the whole encode: the caller of the hot path (src/main.cpp:1930-2743, the round loop and the post-fit BC path,
+ * with the reference's defaults, src/options.h:82-163) ---- */
+typedef struct nntc_b200_encode_args
+{
+    int k;                 /* subtexel sites per texel (--k 4) */
+    int rounds;            /* --rounds 20 */
+    double tol;            /* --tol 1e-4 */
+    int q1_start;          /* --q1-start 3 */
+    int q1_sweeps;         /* --q1-sweeps 4 */
+    int range_pct;         /* --q1-range pct (1) or minmax (0) */
+    double ridge;          /* --ridge 1e-4 */
+    int sweeps;            /* --sweeps 2 (palette mode) */
+    int init_pca;          /* --init pca (1) or box (0) */
+    int bc_refine;         /* --bc-refine 4 */
+    int bc_refine_after;   /* --bc-refine-after 0 */
+    int bc_outer;          /* --bc-outer 2 */
+    float luma[3];         /* 0.299, 0.587, 0.114 */
+} nntc_b200_encode_args;
+
+typedef struct nntc_b200_encode_result
+{
+    int rounds_used;
+    int stop;              /* 0 budget, 1 no-move, 2 tol */
+    int outer_taken;
+    double e_init, e_after_rounds, e_ship;         /* the objective before block (a), after the loop, shipped */
+    double centre_mse, sampled_mse;
+    double psnr[6];        /* per texture: 8-bit decode at the base plane's texel centres vs the source bytes */
+    double ms_a, ms_b, ms_c, ms_e, ms_pack, ms_refine, ms_total;   /* CUDA-event spans of each kind of block */
+    long long objective_passes;
+} nntc_b200_encode_result;
+
+void nntc_b200_encode_defaults(nntc_b200_encode_args* a);
+/* The encode on a device model whose source chain is already resident (device_create). m carries the layout and is
+ * reset to the start state; on return it holds the fitted decoder and grids. k0 / k1 (per plane, optional) receive the
+ * final indices; ep / sel (per plane, optional, bc8) the final endpoints and selectors. */
+int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_args* a,
+                               const double* per_site, nntc_b200_encode_result* r, uint8_t* const* k0,
+                               uint8_t* const* k1, uint8_t* const* ep, uint8_t* const* sel);
 
 /* ---- probes: what the reference's per-kernel harness reads (src/backend_check_probe.h:20-37) ---- */
 int nntc_b200_probe_normal_equations(nntc_b200_device* d, double* out, size_t n);

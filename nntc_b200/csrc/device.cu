@@ -293,6 +293,19 @@ int nntc_b200_version(void)
     return 1;
 }
 
+int nntc_b200_abi_sizes(size_t* out, int n)
+{
+    const size_t sizes[] = { sizeof(nntc_b200_model),         sizeof(nntc_b200_device_info),
+                             sizeof(nntc_b200_plane_report),  sizeof(nntc_b200_level0_report),
+                             sizeof(nntc_b200_objective),     sizeof(nntc_b200_init1_report),
+                             sizeof(nntc_b200_init0_report),  sizeof(nntc_b200_bc_report),
+                             sizeof(nntc_b200_encode_args),   sizeof(nntc_b200_encode_result) };
+    const int count = (int)(sizeof(sizes) / sizeof(sizes[0]));
+    for (int i = 0; i < count && i < n; i++)
+        out[i] = sizes[i];
+    return count < n ? count : n;
+}
+
 int nntc_b200_device_select(int index, nntc_b200_device_info* info)
 {
     std::memset(info, 0, sizeof(*info));

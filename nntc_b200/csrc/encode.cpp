@@ -1,0 +1,459 @@
+// encode.cpp: the whole encode over the C ABI, the caller of the hot path.
+//
+// The round loop and the post-fit BC path of the reference's encoder (src/main.cpp:1930-2743), with its semantics:
+// initialise both latents (level 1 by the box or pca rule, level 0 from the residual one channel at a time, each seed
+// followed by a refit of the decoder); then rounds of (a) decoder, (b) level 1, (c') / (c) level 0, each followed by
+// the objective, freezing both grids at --q1-start and switching to the quantised sweeps; the no-move and the
+// two-consecutive-tol stops; the final sweeps or snaps; then under --l0 bc8 the seed pack, its refinement, the level-1
+// and decoder refit, and up to --bc-outer repack passes accepted only when the shipped E falls (a rejected pass is
+// restored exactly, src/main.cpp:2557-2668). The reporting, the asset writer and the option parsing stay with the
+// host that calls this; what is returned is the model and the per-phase times.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+
+namespace
+{
+
+constexpr double E_REL = 1e-6, E_NOISE = 1e-8;   // src/main.cpp:371-372 (the rise warning, not a decision)
+
+struct Planes8
+{
+    std::vector<std::vector<uint8_t>> buf;
+    std::vector<uint8_t*> ptr;
+    void size(const nntc_b200_model& m, int level, int c)
+    {
+        buf.assign((size_t)m.nplanes, std::vector<uint8_t>());
+        ptr.assign((size_t)m.nplanes, nullptr);
+        for (int i = 0; i < m.nplanes; i++)
+        {
+            const size_t n = level == 0 ? (size_t)m.w0[i] * m.h0[i] * c : (size_t)m.w1[i] * m.h1[i] * c;
+            buf[(size_t)i].assign(n, 0);
+            ptr[(size_t)i] = buf[(size_t)i].data();
+        }
+    }
+};
+
+}   // namespace
+
+using namespace nb;
+
+extern "C"
+{
+
+void nntc_b200_encode_defaults(nntc_b200_encode_args* a)
+{
+    std::memset(a, 0, sizeof(*a));
+    a->k = 4;
+    a->rounds = 20;
+    a->tol = 1e-4;
+    a->q1_start = 3;
+    a->q1_sweeps = 4;
+    a->range_pct = 1;
+    a->ridge = 1e-4;
+    a->sweeps = 2;
+    a->init_pca = 0;
+    a->bc_refine = 4;
+    a->bc_refine_after = 0;
+    a->bc_outer = 2;
+    a->luma[0] = 0.299f;
+    a->luma[1] = 0.587f;
+    a->luma[2] = 0.114f;
+}
+
+int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_args* a,
+                               const double* per_site, nntc_b200_encode_result* r, uint8_t* const* k0_out,
+                               uint8_t* const* k1_out, uint8_t* const* ep_out, uint8_t* const* sel_out)
+{
+    *r = nntc_b200_encode_result{};
+    const int np = m->nplanes, k = a->k;
+    const bool bc8 = m->l0_bc8 != 0;
+    cudaEvent_t t0, t1;
+    NB_CUDA(cudaEventCreate(&t0));
+    NB_CUDA(cudaEventCreate(&t1));
+    NB_CUDA(cudaEventRecord(t0, d->stream));
+    const long long passes0 = nntc_b200_objective_passes();
+
+    // The start state (src/main.cpp:1838-1915): no decoder (the device's is zero), level 0's grid [-1, 1] under bc8,
+    // no level-1 grid yet.
+    std::memset(m->dec_w, 0, sizeof(m->dec_w));
+    std::memset(m->dec_b, 0, sizeof(m->dec_b));
+    m->has_decoder = 1;
+    NB_TRY(nntc_b200_upload_decoder(d, m));
+    m->has_decoder = 0;
+    if (bc8)
+    {
+        m->has_lo0 = 1;
+        for (int c = 0; c < m->c0; c++)
+        {
+            m->lo0[c] = -1.0f;
+            m->hi0[c] = 1.0f;
+        }
+    }
+    m->has_lo1 = 0;
+
+    Planes8 k0, k1;
+    k0.size(*m, 0, m->c0);
+    k1.size(*m, 1, m->c1);
+    nntc_b200_objective e{};
+    double ms = 0.0;
+    auto objective = [&](nntc_b200_objective& out) {
+        const int st = nntc_b200_objective_eval(d, m, k, per_site, &out);
+        r->ms_e += out.ms;
+        return st;
+    };
+    auto block_a = [&]() {
+        double t = 0.0;
+        const int st = nntc_b200_solve_decoder(d, m, k, per_site, &t);
+        r->ms_a += t;
+        return st;
+    };
+
+    // ---- initialisation (src/main.cpp:1930-2122)
+    NB_TRY(nntc_b200_init_level0(d, m, a->luma, m->init0_residual ? 0 : 1, k0.ptr.data()));
+    nntc_b200_init1_report irep{};
+    NB_TRY(nntc_b200_init_level1(d, m, a->init_pca, &irep, k1.ptr.data()));
+    if (!a->init_pca)
+    {
+        // The box init takes the source channels in order with every exact copy of an earlier channel moved to the
+        // back (src/main.cpp:1938-2012); where that changes which channels are taken, level 1 is re-formed from them.
+        const int nout = m->nout, taken = m->c1 < nout ? m->c1 : nout;
+        std::vector<std::vector<float>> src((size_t)np);
+        for (int i = 0; i < np; i++)
+        {
+            src[(size_t)i].resize((size_t)m->w0[i] * m->h0[i] * nout);
+            NB_TRY(download(d, src[(size_t)i].data(), d->planes[(size_t)i].src, src[(size_t)i].size() * sizeof(float)));
+        }
+        std::vector<int> order, copies;
+        for (int s = 0; s < nout; s++)
+        {
+            bool copy = false;
+            for (int e2 = 0; e2 < s && !copy; e2++)
+            {
+                bool same = true;
+                for (int i = 0; i < np && same; i++)
+                    for (size_t t = 0; t < src[(size_t)i].size() / (size_t)nout && same; t++)
+                        same = src[(size_t)i][t * nout + s] == src[(size_t)i][t * nout + e2];
+                copy = same;
+            }
+            (copy ? copies : order).push_back(s);
+        }
+        order.insert(order.end(), copies.begin(), copies.end());
+        std::vector<int> chosen(order.begin(), order.begin() + taken);
+        std::sort(chosen.begin(), chosen.end());
+        bool plain = true;
+        for (int c = 0; c < taken; c++)
+            plain = plain && chosen[(size_t)c] == c;
+        if (!plain)
+        {
+            for (int i = 0; i < np; i++)
+            {
+                const int w0 = m->w0[i], h0 = m->h0[i], w1 = m->w1[i], h1 = m->h1[i];
+                std::vector<float> v1((size_t)w1 * h1 * m->c1);
+                for (int y = 0; y < h1; y++)
+                    for (int x = 0; x < w1; x++)
+                    {
+                        int xa = (int)((long long)x * w0 / w1), xb = (int)((long long)(x + 1) * w0 / w1);
+                        int ya = (int)((long long)y * h0 / h1), yb = (int)((long long)(y + 1) * h0 / h1);
+                        xb = std::min(w0, xb <= xa ? xa + 1 : xb);
+                        yb = std::min(h0, yb <= ya ? ya + 1 : yb);
+                        for (int c = 0; c < m->c1; c++)
+                        {
+                            const size_t t1 = (size_t)y * w1 + x;
+                            if (c >= nout)
+                            {
+                                v1[t1 * m->c1 + c] = 0.0f;
+                                continue;
+                            }
+                            const int sc = order[(size_t)c];
+                            float acc = 0.0f;
+                            int n = 0;
+                            for (int sy = ya; sy < yb; sy++)
+                                for (int sx = xa; sx < xb; sx++)
+                                {
+                                    acc += src[(size_t)i][((size_t)sy * w0 + sx) * nout + sc];
+                                    n++;
+                                }
+                            const float inv = n > 0 ? 1.0f / (float)n : 0.0f;
+                            v1[t1 * m->c1 + c] = 2.0f * acc * inv - 1.0f;
+                        }
+                    }
+                NB_TRY(nntc_b200_level1_upload(d, i, v1.data(), v1.size()));
+            }
+            NB_TRY(nntc_b200_quantise_level1(d, m, 0, k1.ptr.data()));
+        }
+    }
+    NB_TRY(objective(e));
+    r->e_init = e.e;
+    NB_TRY(block_a());
+    NB_TRY(objective(e));
+    if (m->init0_residual)
+        for (int c = 0; c < m->c0; c++)
+        {
+            nntc_b200_init0_report crep{};
+            NB_TRY(nntc_b200_init0_residual_channel(d, m, c, per_site, &crep, k0.ptr.data()));
+            NB_TRY(objective(e));
+            NB_TRY(block_a());
+            NB_TRY(objective(e));
+            if (!bc8)
+            {
+                std::vector<nntc_b200_level0_report> l0((size_t)np);
+                NB_TRY(nntc_b200_solve_level0_all(d, m, k, a->sweeps, l0.data(), &ms));
+                r->ms_c += ms;
+                NB_TRY(block_a());
+                NB_TRY(objective(e));
+            }
+        }
+
+    // ---- the round loop (src/main.cpp:2165-2390)
+    std::vector<nntc_b200_plane_report> lr((size_t)np), lr0((size_t)np);
+    bool frozen = false;
+    int tol_hits = 0;
+    double e_prev = e.e;
+    for (int round = 1; round <= a->rounds; round++)
+    {
+        nntc_b200_objective ea{}, eb{}, ec{};
+        NB_TRY(block_a());
+        NB_TRY(objective(ea));
+        if (a->q1_start > 0 && round >= a->q1_start && !frozen)
+        {
+            NB_TRY(nntc_b200_freeze_level1_grid(d, m, a->range_pct, k1.ptr.data()));
+            if (bc8)
+                NB_TRY(nntc_b200_freeze_level0_grid(d, m, a->range_pct, k0.ptr.data()));
+            frozen = true;
+        }
+        if (frozen)
+            NB_TRY(nntc_b200_sweep_level1_all(d, m, k, a->ridge, a->q1_sweeps, lr.data(), &ms));
+        else
+            NB_TRY(nntc_b200_solve_level1_all(d, m, k, a->ridge, lr.data(), &ms));
+        r->ms_b += ms;
+        long long moved1 = 0;
+        double delta2 = 0.0, plane2 = 0.0;
+        for (int p = 0; p < np; p++)
+        {
+            moved1 += lr[(size_t)p].quantised ? lr[(size_t)p].moved : lr[(size_t)p].moved_values;
+            delta2 += lr[(size_t)p].delta2;
+            plane2 += lr[(size_t)p].plane2;
+        }
+        NB_TRY(objective(eb));
+        long long moved0 = 0;
+        if (bc8)
+        {
+            if (frozen)
+                NB_TRY(nntc_b200_sweep_level0_cont_all(d, m, k, a->ridge, a->q1_sweeps, lr0.data(), &ms));
+            else
+                NB_TRY(nntc_b200_solve_level0_cont_all(d, m, k, a->ridge, lr0.data(), &ms));
+            for (int p = 0; p < np; p++)
+                moved0 += lr0[(size_t)p].quantised ? lr0[(size_t)p].moved : lr0[(size_t)p].moved_values;
+        }
+        else
+        {
+            std::vector<nntc_b200_level0_report> l0((size_t)np);
+            NB_TRY(nntc_b200_solve_level0_all(d, m, k, a->sweeps, l0.data(), &ms));
+            for (int p = 0; p < np; p++)
+                moved0 += l0[(size_t)p].moved_total;
+        }
+        r->ms_c += ms;
+        NB_TRY(objective(ec));
+        (void)E_REL;
+        (void)E_NOISE;
+        r->rounds_used = round;
+        const double drop = ec.e > 0.0 ? (e_prev - ec.e) / ec.e : 0.0;
+        e_prev = ec.e;
+        const double dn = std::sqrt(delta2), pn = std::sqrt(plane2);
+        const bool level1_still = frozen ? moved1 == 0 : dn <= 1e-7 * (pn > 0.0 ? pn : 1.0);
+        if (moved0 == 0 && level1_still)
+        {
+            r->stop = 1;
+            break;
+        }
+        tol_hits = drop < a->tol ? tol_hits + 1 : 0;
+        if (tol_hits >= 2)
+        {
+            r->stop = 2;
+            break;
+        }
+    }
+    if (frozen)
+        NB_TRY(nntc_b200_sweep_level1_all(d, m, k, a->ridge, a->q1_sweeps, lr.data(), &ms));
+    else
+        NB_TRY(nntc_b200_quantise_level1(d, m, a->range_pct, k1.ptr.data()));
+    r->ms_b += frozen ? ms : 0.0;
+    if (bc8)
+    {
+        if (frozen)
+        {
+            NB_TRY(nntc_b200_sweep_level0_cont_all(d, m, k, a->ridge, a->q1_sweeps, lr0.data(), &ms));
+            r->ms_c += ms;
+        }
+        else
+            NB_TRY(nntc_b200_quantise_level0(d, m, a->range_pct, k0.ptr.data()));
+    }
+    else
+    {
+        std::vector<nntc_b200_level0_report> l0((size_t)np);
+        NB_TRY(nntc_b200_solve_level0_all(d, m, k, a->sweeps, l0.data(), &ms));
+        r->ms_c += ms;
+    }
+    NB_TRY(block_a());
+    for (int i = 0; i < np; i++)
+        NB_TRY(nntc_b200_level0_download(d, i, k0.ptr[(size_t)i], k0.buf[(size_t)i].size()));
+    NB_TRY(objective(e));
+    r->e_after_rounds = e.e;
+
+    // ---- the post-fit BC path (src/main.cpp:2485-2694)
+    if (bc8)
+    {
+        auto refit_level1 = [&]() {
+            const int st = nntc_b200_sweep_level1_all(d, m, k, a->ridge, a->q1_sweeps, lr.data(), &ms);
+            r->ms_b += ms;
+            return st;
+        };
+        nntc_b200_objective probe{};
+        NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, (const uint8_t* const*)k0.ptr.data(), &ms));
+        r->ms_pack += ms;
+        std::vector<nntc_b200_bc_report> rp((size_t)(a->bc_refine > 0 ? a->bc_refine : 1));
+        NB_TRY(nntc_b200_bc_refine(d, m, a->bc_refine, rp.data(), &ms));
+        r->ms_refine += ms;
+        NB_TRY(refit_level1());
+        NB_TRY(block_a());
+        NB_TRY(objective(probe));
+        if (a->bc_refine_after > 0)
+        {
+            NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 0, nullptr, &ms));
+            r->ms_pack += ms;
+            std::vector<nntc_b200_bc_report> ra((size_t)a->bc_refine_after);
+            NB_TRY(nntc_b200_bc_refine(d, m, a->bc_refine_after, ra.data(), &ms));
+            r->ms_refine += ms;
+            NB_TRY(objective(probe));
+        }
+        double e_ship = probe.e;
+        for (int pass = 1; pass <= a->bc_outer; pass++)
+        {
+            // Everything a rejected pass would leave behind, kept (src/main.cpp:2561-2590).
+            std::vector<std::vector<float>> keep_v0((size_t)np), keep_v1((size_t)np);
+            std::vector<std::vector<uint8_t>> keep_k0((size_t)np), keep_k1((size_t)np), keep_ep((size_t)np),
+                keep_sel((size_t)np);
+            std::vector<uint8_t*> pe((size_t)np), ps((size_t)np);
+            for (int i = 0; i < np; i++)
+            {
+                const DevPlane& p = d->planes[(size_t)i];
+                keep_v0[(size_t)i].resize((size_t)p.w0 * p.h0 * m->c0);
+                keep_v1[(size_t)i].resize((size_t)p.w1 * p.h1 * m->c1);
+                keep_k0[(size_t)i].resize(keep_v0[(size_t)i].size());
+                keep_k1[(size_t)i].resize(keep_v1[(size_t)i].size());
+                keep_ep[(size_t)i].resize(p.blocks() * m->c0 * 2);
+                keep_sel[(size_t)i].resize(p.blocks() * m->c0 * 16);
+                pe[(size_t)i] = keep_ep[(size_t)i].data();
+                ps[(size_t)i] = keep_sel[(size_t)i].data();
+                NB_TRY(nntc_b200_level0_download_values(d, i, keep_v0[(size_t)i].data(), keep_v0[(size_t)i].size()));
+                NB_TRY(nntc_b200_level0_download(d, i, keep_k0[(size_t)i].data(), keep_k0[(size_t)i].size()));
+                NB_TRY(nntc_b200_level1_download(d, i, keep_v1[(size_t)i].data(), keep_v1[(size_t)i].size()));
+                NB_TRY(nntc_b200_level1_download_indices(d, i, keep_k1[(size_t)i].data(), keep_k1[(size_t)i].size()));
+            }
+            NB_TRY(nntc_b200_bc_state_save(d, m, pe.data(), ps.data()));
+            const nntc_b200_model keep_m = *m;
+            const Planes8 keep_mk0 = k0, keep_mk1 = k1;
+
+            NB_TRY(refit_level1());
+            NB_TRY(block_a());
+            if (frozen)
+                NB_TRY(nntc_b200_sweep_level0_cont_all(d, m, k, a->ridge, a->q1_sweeps, lr0.data(), &ms));
+            else
+            {
+                NB_TRY(nntc_b200_solve_level0_cont_all(d, m, k, a->ridge, lr0.data(), &ms));
+                NB_TRY(nntc_b200_snap_level0_on_grid(d, m, k0.ptr.data()));
+            }
+            r->ms_c += ms;
+            for (int i = 0; i < np; i++)
+                NB_TRY(nntc_b200_level0_download(d, i, k0.ptr[(size_t)i], k0.buf[(size_t)i].size()));
+            NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, (const uint8_t* const*)k0.ptr.data(), &ms));
+            r->ms_pack += ms;
+            NB_TRY(nntc_b200_bc_refine(d, m, a->bc_refine, rp.data(), &ms));
+            r->ms_refine += ms;
+            NB_TRY(objective(probe));
+            if (probe.e < e_ship)
+            {
+                e_ship = probe.e;
+                r->outer_taken++;
+                continue;
+            }
+            for (int i = 0; i < np; i++)
+            {
+                NB_TRY(nntc_b200_level0_upload(d, i, keep_v0[(size_t)i].data(), keep_v0[(size_t)i].size()));
+                NB_TRY(nntc_b200_level0_upload_indices(d, i, keep_k0[(size_t)i].data(), keep_k0[(size_t)i].size()));
+                NB_TRY(nntc_b200_level1_upload(d, i, keep_v1[(size_t)i].data(), keep_v1[(size_t)i].size()));
+                NB_TRY(nntc_b200_level1_upload_indices(d, i, keep_k1[(size_t)i].data(), keep_k1[(size_t)i].size()));
+            }
+            k0 = keep_mk0;
+            k1 = keep_mk1;
+            for (int i = 0; i < np; i++)
+            {
+                k0.ptr[(size_t)i] = k0.buf[(size_t)i].data();
+                k1.ptr[(size_t)i] = k1.buf[(size_t)i].data();
+            }
+            NB_TRY(nntc_b200_bc_state_restore(d, m, (const uint8_t* const*)pe.data(), (const uint8_t* const*)ps.data()));
+            *m = keep_m;
+            NB_TRY(nntc_b200_upload_decoder(d, m));
+            NB_TRY(nntc_b200_upload_grids(d, m));
+            break;
+        }
+        NB_TRY(refit_level1());
+        NB_TRY(block_a());
+    }
+
+    nntc_b200_objective shipped{};
+    NB_TRY(objective(shipped));
+    r->e_ship = shipped.e;
+    r->centre_mse = shipped.centre_mse;
+    r->sampled_mse = shipped.sampled_mse;
+    NB_CUDA(cudaEventRecord(t1, d->stream));
+    NB_CUDA(cudaEventSynchronize(t1));
+    float total = 0.0f;
+    NB_CUDA(cudaEventElapsedTime(&total, t0, t1));
+    r->ms_total = total;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    r->objective_passes = nntc_b200_objective_passes() - passes0;
+
+    // The per-texture 8-bit PSNR of the base level against the source bytes (src/main.cpp:2743, 3000-3060).
+    {
+        const DevPlane& p = d->planes[0];
+        const size_t n = (size_t)p.w0 * p.h0;
+        std::vector<uint8_t> rgb(n * m->nout);
+        std::vector<float> src(n * m->nout);
+        NB_TRY(nntc_b200_decode_plane(d, m, 0, rgb.data(), rgb.size()));
+        NB_TRY(download(d, src.data(), p.src, src.size() * sizeof(float)));
+        for (int t = 0; t < m->textures && t < 6; t++)
+        {
+            double se = 0.0;
+            for (size_t i = 0; i < n; i++)
+                for (int c = 0; c < 3; c++)
+                {
+                    const double want = std::lround((double)src[i * m->nout + 3 * t + c] * 255.0);
+                    const double e2 = (double)rgb[i * m->nout + 3 * t + c] - want;
+                    se += e2 * e2;
+                }
+            const double mse = se / (double)(n * 3);
+            r->psnr[t] = mse > 0.0 ? 10.0 * std::log10(255.0 * 255.0 / mse) : 99.0;
+        }
+    }
+    for (int i = 0; i < np; i++)
+    {
+        if (k0_out && k0_out[i])
+            NB_TRY(nntc_b200_level0_download(d, i, k0_out[i], (size_t)m->w0[i] * m->h0[i] * m->c0));
+        if (k1_out && k1_out[i])
+            NB_TRY(nntc_b200_level1_download_indices(d, i, k1_out[i], (size_t)m->w1[i] * m->h1[i] * m->c1));
+    }
+    if (bc8 && ((ep_out && ep_out[0]) || (sel_out && sel_out[0])))
+        NB_TRY(nntc_b200_bc_state_save(d, m, ep_out, sel_out));
+    return NNTC_B200_OK;
+}
+
+}   // extern "C"
