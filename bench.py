@@ -1,0 +1,334 @@
+"""Encode throughput of the B200 NNTC encoder hot path: one step = one whole encode of the workload material.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
+
+Metric: encode Mpix/s = base W x H of the material / encode seconds (the reference's `time ... s total` definition,
+src/main.cpp:1788-2948, with the base extent). N > 1 runs under torchrun as REPLICAS: every rank encodes its own
+seeded material of the same configuration on its own GPU, with no collective on the data path (the encode does not
+shard; one material per GPU); the whole-job value is the pixels of every rank over the slowest rank's time.
+
+- `value`: the encode on a device model whose source chain is already resident in HBM, timed by the library's CUDA
+  events on its own stream around the whole encode (nntc_b200_encode_result.ms_total), K steps bracketed by a barrier
+  and a synchronize, max over ranks.
+- `e2e`: the same through the C ABI with host buffers: device_create (the chain's H2D copy from pinned host memory),
+  the encode, and the D2H read of its result (indices, BC endpoints/selectors, decoder) every step.
+- `roofline`: the dominant kernel's achieved rate from per-launch CUDA events over the timed steps
+  (nntc_b200_kernel_stats), against MEASURED_PEAKS.json.
+- `cpu_baseline`: the reference's own CPU encoder (oracle/_ref/nntc_encode_cpu, built from the reference sources) on
+  a bounded crop of the same material, on this host's cores.
+- `--impl reference`: that reference CPU encoder alone, timed per step on the crop (rank 0; other ranks exit 0).
+The inputs are seeded synthetic textures with the shapes of the configuration (nntc_b200/materials.py); every step's
+working set is far larger than the 126 MB L2, so no flush is needed between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from nntc_b200 import abi, check, lib, materials  # noqa: E402
+
+# Per-unit figures of the dominant kernels (DESIGN.md states their derivation): bytes a launch must move at least.
+CONFIG_NAMES = {0: "1x256x256 noise+rects c0=2 c1=4", 1: "4x512x512 pbr c0=2 c1=4", 2: "4x1024x1024 pbr c0=2 c1=4",
+                3: "4x2048x1024 pbr c0=4 c1=4", 4: "6x4096x4096 pbr c0=4 c1=4"}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        load = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def crop_material(mat, size):
+    tex = [t[:size, :size].copy() for t in mat.textures]
+    return materials.Material(f"{size}x{size} crop of {mat.name}", tex, mat.c0, mat.c1, mat.k).build()
+
+
+def reference_cpu(mat, steps, warmup, threads):
+    """The reference's CPU encoder on `mat` (PNG inputs), each run's own `time ... s total` (Mpix/s of the base)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "nntc_encode_cpu")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/nntc_encode_cpu is not built"
+    tmp = tempfile.mkdtemp(prefix="nntc_ref_")
+    pngs = materials.save_material(mat, os.path.join(tmp, "in"))
+    cmd = [exe, *pngs, "-o", os.path.join(tmp, "out") + "/", "--backend", "cpu", "--c0", str(mat.c0), "--c1",
+           str(mat.c1), "-j", str(threads), "--quiet"]
+    secs = []
+    for i in range(warmup + steps):
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            return None, "reference encoder failed: " + (p.stdout + p.stderr)[-300:]
+        m = re.search(r"time\s+([\d.]+) s total", p.stdout)
+        if i >= warmup:
+            secs.append(float(m.group(1)))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return secs, None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    mat = crop_material(materials.config(args.config, seed=0) if args.config != 4 else big_material(0), args.crop)
+    threads = os.cpu_count() or 1
+    secs, err = reference_cpu(mat, args.steps, args.warmup, threads)
+    if err:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    mpix = mat.width * mat.height / 1e6
+    value = mpix * len(secs) / sum(secs)
+    sample = f"{mat.name} (a {args.crop}x{args.crop} crop of the workload), whole encode, {threads} threads"
+    print(json.dumps({
+        "impl": "reference", "metric": "encode Mpix/s", "value": round(value, 6), "unit": "Mpix/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * sum(secs) / len(secs), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": CONFIG_NAMES[args.config], "sample": sample},
+        "cpu_baseline": {"value": round(value, 6), "unit": "Mpix/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 6), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def big_material(seed):
+    return materials.config(4, seed=seed)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=4)
+    ap.add_argument("--crop", type=int, default=256, help="edge of the CPU-baseline crop")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    mat = materials.config(args.config, seed=rank) if args.config != 4 else big_material(rank)
+    model = abi.make_model(mat)
+    L = lib()
+    ea = abi.EncodeArgs()
+    L.nntc_b200_encode_defaults(C.byref(ea))
+    per_site = (C.c_double * len(mat.per_site))(*mat.per_site)
+    # pinned host copies of the source chain (what the e2e leg copies to the device every step)
+    pinned = [torch.from_numpy(np.ascontiguousarray(c, np.float32)).pin_memory() for c in mat.chain]
+    chain_ptrs = (C.POINTER(C.c_float) * len(pinned))(*[C.cast(t.data_ptr(), C.POINTER(C.c_float)) for t in pinned])
+    h2d = sum(t.numel() * 4 for t in pinned)
+
+    def outputs():
+        k0 = [np.zeros(p[0] * p[1] * mat.c0, np.uint8) for p in mat.planes]
+        k1 = [np.zeros(p[2] * p[3] * mat.c1, np.uint8) for p in mat.planes]
+        ep = [np.zeros(((p[0] + 3) // 4) * ((p[1] + 3) // 4) * mat.c0 * 2, np.uint8) for p in mat.planes]
+        sel = [np.zeros(e.size * 8, np.uint8) for e in ep]
+        return k0, k1, ep, sel
+
+    out = outputs()
+    d2h = sum(a.size for grp in out for a in grp) + (model.nout * (model.nin + 1)) * 4
+
+    handle = C.c_void_p()
+    check(L.nntc_b200_device_create(C.byref(model), chain_ptrs, C.byref(handle)), "device_create")
+
+    def encode_resident():
+        r = abi.EncodeResult()
+        m = abi.make_model(mat)
+        check(L.nntc_b200_encode_on_device(handle, C.byref(m), C.byref(ea), per_site, C.byref(r), None, None, None,
+                                           None), "encode")
+        return r
+
+    for _ in range(args.warmup):
+        encode_resident()
+    check(L.nntc_b200_kernel_timing(handle, 1), "timing")
+    check(L.nntc_b200_kernel_stats(handle, 0, None, None, 1), "reset")
+    launches0 = L.nntc_b200_launch_count()
+    results = []
+    with Clocks(local) as clocks:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            results.append(encode_resident())
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        if world > 1:
+            dist.barrier()
+    launches = L.nntc_b200_launch_count() - launches0
+    device_ms = sum(r.ms_total for r in results)
+    stats = {}
+    for kid, name in enumerate(["objective", "normal_equations", "assemble_level1", "assemble_level0", "cg_matvec",
+                                "quant_sweep", "bc_refine"]):
+        n = C.c_longlong()
+        ms = C.c_double()
+        check(L.nntc_b200_kernel_stats(handle, kid, C.byref(n), C.byref(ms), 0), "stats")
+        stats[name] = (n.value, ms.value)
+    check(L.nntc_b200_kernel_timing(handle, 0), "timing")
+
+    # e2e: through the C ABI with host buffers, every step's H2D of the chain and D2H of the result included
+    e2e_ms = []
+    if world > 1:
+        dist.barrier()
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        h = C.c_void_p()
+        m = abi.make_model(mat)
+        check(L.nntc_b200_device_create(C.byref(m), chain_ptrs, C.byref(h)), "device_create")
+        r = abi.EncodeResult()
+        k0, k1, ep, sel = out
+        check(L.nntc_b200_encode_on_device(h, C.byref(m), C.byref(ea), per_site, C.byref(r), abi.u8_ptrs(k0),
+                                           abi.u8_ptrs(k1), abi.u8_ptrs(ep), abi.u8_ptrs(sel)), "encode")
+        L.nntc_b200_device_destroy(h)
+        ev1.record()
+        ev1.synchronize()
+        e2e_ms.append(ev0.elapsed_time(ev1))
+    L.nntc_b200_device_destroy(handle)
+
+    mine = torch.tensor([device_ms, sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(mine, op=dist.ReduceOp.MAX)
+    device_ms, e2e_total = mine.tolist()
+    mpix = mat.width * mat.height / 1e6
+    value = world * mpix * args.steps / (device_ms / 1000.0)
+    e2e_value = world * mpix * args.steps / (e2e_total / 1000.0)
+
+    if rank == 0:
+        hbm, tf, src = peaks()
+        dom = max(stats, key=lambda k: stats[k][1])
+        roof = roofline(dom, stats[dom], mat, hbm, tf, src)
+        line = {
+            "metric": "encode Mpix/s", "value": round(value, 6), "unit": "Mpix/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(device_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded, nntc_b200/materials.py)",
+            "config": {"workload": CONFIG_NAMES[args.config], "base": [mat.width, mat.height],
+                       "textures": len(mat.textures), "c0": mat.c0, "c1": mat.c1, "k": mat.k,
+                       "chain_pixels": mat.chain_pixels, "parallelism": f"replicas x{world}",
+                       "l2": "working set > 126 MB L2 every step, no flush needed",
+                       "psnr": [round(x, 3) for x in results[-1].psnr[: len(mat.textures)]],
+                       "rounds": results[-1].rounds_used, "wall_s_per_step": round(wall / args.steps, 3),
+                       "phase_ms": {k: round(getattr(results[-1], "ms_" + k), 2) for k in
+                                    ("a", "b", "c", "e", "pack", "refine", "total")},
+                       "kernel_ms": {k: [v[0], round(v[1], 2)] for k, v in stats.items()}},
+            "e2e": {"value": round(e2e_value, 6), "unit": "Mpix/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "clocks": clocks.summary(),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            crop = crop_material(mat, args.crop)
+            secs, err = reference_cpu(crop, 1, 0, os.cpu_count() or 1)
+            line["cpu_baseline"] = ({"unavailable": err} if err else {
+                "value": round(crop.width * crop.height / 1e6 / secs[0], 6), "unit": "Mpix/s",
+                "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"{args.crop}x{args.crop} crop of the workload ({len(mat.textures)} textures, c0 {mat.c0} "
+                          f"c1 {mat.c1}), whole encode by the reference CPU encoder, one run"})
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def roofline(name, stat, mat, hbm, tf, src):
+    """The dominant kernel against the HBM roofline: its algorithmic bytes per launch over its mean launch time."""
+    launches, ms = stat
+    if launches == 0:
+        return None
+    per = algorithmic_bytes(name, mat)
+    achieved = per / (ms / launches / 1000.0) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": src,
+            "bytes_per_launch": per, "launches": launches, "ms_per_launch": round(ms / launches, 4)}
+
+
+def algorithmic_bytes(name, mat):
+    """Bytes a launch must read and write at least (every plane of the chain), the figures DESIGN.md derives."""
+    c0, c1, nout = mat.c0, mat.c1, 3 * len(mat.textures)
+    t0 = sum(p[0] * p[1] for p in mat.planes)
+    t1 = sum(p[2] * p[3] for p in mat.planes)
+    if name == "assemble_level0":   # reads src, v0 (and v1), writes the FP64 stencil and gradient
+        return t0 * (4 * nout + 4 * c0 + 5 * c0 * c0 * 8 + 8 * c0) + t1 * 4 * c1
+    if name == "assemble_level1":
+        return t0 * (4 * nout + 4 * c0) + t1 * (4 * c1 + 5 * c1 * c1 * 8 + 8 * c1)
+    if name == "objective" or name == "normal_equations":
+        return t0 * (4 * nout + 4 * c0) + t1 * 4 * c1
+    if name == "cg_matvec":   # the larger of the two unknowns' stencils: own 5 blocks + x in + y out
+        return max(t0 * (5 * c0 * c0 * 8 + 3 * 8 * c0), t1 * (5 * c1 * c1 * 8 + 3 * 8 * c1))
+    if name == "quant_sweep":   # one colour: a quarter of the texels read their 9 blocks' worth
+        return max(t0 * (5 * c0 * c0 * 8 + 2 * 8 * c0 + 9 * c0) // 4 * 4 // 4, t1 * (5 * c1 * c1 * 8) // 4)
+    if name == "bc_refine":   # one colour: a quarter of the blocks read their stencil, grad, planes
+        return t0 * (5 * c0 * c0 * 8 + 8 * c0 + 4 * c0 + 4 * c0 + 8 * c0) // 4
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -268,6 +268,26 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
                                const double* per_site, nntc_b200_encode_result* r, uint8_t* const* k0,
                                uint8_t* const* k1, uint8_t* const* ep, uint8_t* const* sel);
 
+/* ---- measurement ---- */
+/* Kernels this library has launched since the process started (every launch, every device). */
+long long nntc_b200_launch_count(void);
+/* The hot kernels whose launches can be timed individually with CUDA events on the library's own stream. */
+enum nntc_b200_kernel
+{
+    NNTC_B200_K_OBJECTIVE = 0,   /* the objective over every site of every plane */
+    NNTC_B200_K_NORMAL_EQ,       /* block (a)'s normal equations */
+    NNTC_B200_K_ASSEMBLE1,       /* block (b)'s stencil and gradient gather */
+    NNTC_B200_K_ASSEMBLE0,       /* block (c')'s stencil and gradient gather */
+    NNTC_B200_K_MATVEC,          /* one conjugate-gradient stencil mat-vec over every plane */
+    NNTC_B200_K_SWEEP,           /* one colour of the quantised sweeps */
+    NNTC_B200_K_REFINE,          /* one colour of the BC refinement */
+    NNTC_B200_K_COUNT
+};
+/* on != 0 brackets every launch of the kernels above with a pair of CUDA events; stats accumulate until reset. */
+int nntc_b200_kernel_timing(nntc_b200_device* d, int on);
+/* The launches of `kernel` since the last reset and their summed event time; reset != 0 clears every kernel's. */
+int nntc_b200_kernel_stats(nntc_b200_device* d, int kernel, long long* launches, double* ms, int reset);
+
 /* ---- probes: what the reference's per-kernel harness reads (src/backend_check_probe.h:20-37) ---- */
 int nntc_b200_probe_normal_equations(nntc_b200_device* d, double* out, size_t n);
 int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double* stencil, double* grad,

@@ -108,3 +108,12 @@ def check(status: int, what: str = "") -> None:
     if status != 0:
         msg = lib().nntc_b200_last_error().decode(errors="replace")
         raise NntcError(f"{what}: status {status}: {msg}")
+
+PROTOTYPES.update({
+    "nntc_b200_launch_count": (C.c_longlong, []),
+    "nntc_b200_kernel_timing": (_I, [_P, _I]),
+    "nntc_b200_kernel_stats": (_I, [_P, _I, C.POINTER(C.c_longlong), _PD, _I]),
+})
+
+KERNELS = ["objective", "normal_equations", "assemble_level1", "assemble_level0", "cg_matvec", "quant_sweep",
+           "bc_refine"]

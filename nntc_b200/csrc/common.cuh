@@ -55,7 +55,14 @@ int cuda_status(cudaError_t err, const char* call, const char* file, int line);
             return nb_st_;                                                                                            \
     } while (0)
 
-#define NB_LAUNCHED() NB_CUDA(cudaGetLastError())
+// Every kernel launch is followed by this: it counts the launch (nntc_b200_launch_count) and checks it.
+void count_launch();
+#define NB_LAUNCHED()                                                                                                 \
+    do                                                                                                                \
+    {                                                                                                                 \
+        ::nb::count_launch();                                                                                         \
+        NB_CUDA(cudaGetLastError());                                                                                  \
+    } while (0)
 
 inline int grid_for(size_t n, int threads)
 {

@@ -227,7 +227,9 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     dim3 grid(LS_GRID, (unsigned)P.n);
     const size_t shared = LS_THREADS * sizeof(double) + (size_t)(S.nv + S.nt) * TILE * LS_STRIDE * sizeof(float);
     NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
+    NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
     k_ls_accumulate<<<grid, LS_THREADS, shared, d->stream>>>(P, S, LsArgs{ d->ls_partial, entries });
+    NB_TRY(ktimer_end(d));
     NB_LAUNCHED();
     k_ls_reduce<<<grid_for((size_t)entries, 128), 128, 0, d->stream>>>(d->ls_partial, entries, P.n, omega,
                                                                       d->reduction);

@@ -4,6 +4,7 @@
 // src/solve_level1.cu:1098-1500 / src/solve_level0.cu:329-369, over this library's own single-stream model.
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -51,6 +52,56 @@ int cuda_status(cudaError_t err, const char* call, const char* file, int line)
     return NNTC_B200_ERR_CUDA;
 }
 
+static std::atomic<long long> g_launches{ 0 };
+
+void count_launch()
+{
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+int ktimer_begin(nntc_b200_device* d, int kind)
+{
+    if (!d->ktiming)
+        return NNTC_B200_OK;
+    cudaEvent_t e[2];
+    for (cudaEvent_t& x : e)
+    {
+        if (d->kpool.empty())
+            NB_CUDA(cudaEventCreate(&x));
+        else
+        {
+            x = d->kpool.back();
+            d->kpool.pop_back();
+        }
+    }
+    d->kpending.push_back({ kind, e[0], e[1] });
+    NB_CUDA(cudaEventRecord(e[0], d->stream));
+    return NNTC_B200_OK;
+}
+
+int ktimer_end(nntc_b200_device* d)
+{
+    if (!d->ktiming || d->kpending.empty())
+        return NNTC_B200_OK;
+    NB_CUDA(cudaEventRecord(d->kpending.back().b, d->stream));
+    return NNTC_B200_OK;
+}
+
+int ktimer_harvest(nntc_b200_device* d)
+{
+    for (const nntc_b200_device::Pending& p : d->kpending)
+    {
+        float t = 0.0f;
+        NB_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
+        d->klaunches[p.kind]++;
+        d->kms[p.kind] += (double)t;
+        d->kpool.push_back(p.a);
+        d->kpool.push_back(p.b);
+    }
+    d->kpending.clear();
+    return NNTC_B200_OK;
+}
+
 int block_begin(nntc_b200_device* d)
 {
     NB_CUDA(cudaEventRecord(d->ev[0], d->stream));
@@ -65,7 +116,7 @@ int block_end(nntc_b200_device* d, double* ms)
     NB_CUDA(cudaEventElapsedTime(&t, d->ev[0], d->ev[1]));
     if (ms)
         *ms = (double)t;
-    return NNTC_B200_OK;
+    return ktimer_harvest(d);
 }
 
 int upload(nntc_b200_device* d, void* dst, const void* src, size_t bytes)
@@ -291,6 +342,41 @@ const char* nntc_b200_last_error(void)
 int nntc_b200_version(void)
 {
     return 1;
+}
+
+long long nntc_b200_launch_count(void)
+{
+    return g_launches.load();
+}
+
+int nntc_b200_kernel_timing(nntc_b200_device* d, int on)
+{
+    NB_CUDA(cudaStreamSynchronize(d->stream));
+    NB_TRY(ktimer_harvest(d));
+    d->ktiming = on != 0;
+    return NNTC_B200_OK;
+}
+
+int nntc_b200_kernel_stats(nntc_b200_device* d, int kernel, long long* launches, double* ms, int reset)
+{
+    if (kernel < 0 || kernel >= NNTC_B200_K_COUNT)
+    {
+        set_error(NNTC_B200_ERR_ARG, "no such kernel");
+        return NNTC_B200_ERR_ARG;
+    }
+    NB_CUDA(cudaStreamSynchronize(d->stream));
+    NB_TRY(ktimer_harvest(d));
+    if (launches)
+        *launches = d->klaunches[kernel];
+    if (ms)
+        *ms = d->kms[kernel];
+    if (reset)
+        for (int k = 0; k < NNTC_B200_K_COUNT; k++)
+        {
+            d->klaunches[k] = 0;
+            d->kms[k] = 0.0;
+        }
+    return NNTC_B200_OK;
 }
 
 int nntc_b200_abi_sizes(size_t* out, int n)
@@ -524,6 +610,13 @@ void nntc_b200_device_destroy(nntc_b200_device* d)
         cudaFree(b);
     cudaFreeHost(d->host_scalars);
     cudaFreeHost(d->host_counters);
+    for (const nntc_b200_device::Pending& p : d->kpending)
+    {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (cudaEvent_t e : d->kpool)
+        cudaEventDestroy(e);
     for (cudaEvent_t e : d->ev)
         if (e)
             cudaEventDestroy(e);

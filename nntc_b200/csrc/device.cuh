@@ -121,6 +121,19 @@ struct nntc_b200_device
     size_t bytes = 0;
     int nout = 0, nin = 0, c0 = 0, c1 = 0;
     bool l0_bc8 = false;
+
+    // Per-kernel event timing (nntc_b200_kernel_timing): pairs recorded around each launch of a hot kernel, read back
+    // after the block that launched them has been waited for.
+    struct Pending
+    {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    bool ktiming = false;
+    std::vector<cudaEvent_t> kpool;
+    std::vector<Pending> kpending;
+    long long klaunches[NNTC_B200_K_COUNT] = {};
+    double kms[NNTC_B200_K_COUNT] = {};
 };
 
 namespace nb
@@ -177,6 +190,11 @@ inline Planes planes_for(const nntc_b200_device* d, int level0, F items)
 // Record the span of a block of work on the model's stream and return it in ms after synchronising.
 int block_begin(nntc_b200_device* d);
 int block_end(nntc_b200_device* d, double* ms);
+
+// Brackets of one launch of a hot kernel (no-ops unless kernel timing is on); harvested at every block_end.
+int ktimer_begin(nntc_b200_device* d, int kind);
+int ktimer_end(nntc_b200_device* d);
+int ktimer_harvest(nntc_b200_device* d);
 
 // Upload on the model's stream and wait (the staging buffer is the caller's).
 int upload(nntc_b200_device* d, void* dst, const void* src, size_t bytes);

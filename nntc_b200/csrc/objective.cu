@@ -214,7 +214,9 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
     double* sums = d->obj_partial + (size_t)nblocks * 3;
     ObjArgs A{ d->weights, d->bias, d->cw, d->obj_partial };
     NB_TRY(block_begin(d));
+    NB_TRY(ktimer_begin(d, NNTC_B200_K_OBJECTIVE));
     k_objective<<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, A);
+    NB_TRY(ktimer_end(d));
     NB_LAUNCHED();
     k_objective_reduce<<<P.n, 256, 0, d->stream>>>(P, d->obj_partial, nblocks, sums);
     NB_LAUNCHED();

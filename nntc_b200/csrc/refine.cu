@@ -645,7 +645,9 @@ int bc_refine_passes(nntc_b200_device* d, const nntc_b200_model* m, int passes, 
                 continue;
             RefineArgs R{ d->lo0, d->hi0, cx, cy, d->bc_stats };
             const int grid = grid_for((size_t)P.start[P.n], REFINE_WARPS);
+            NB_TRY(ktimer_begin(d, NNTC_B200_K_REFINE));
             k_bc_refine<<<grid, 32 * REFINE_WARPS, shared, d->stream>>>(P, R);
+            NB_TRY(ktimer_end(d));
             NB_LAUNCHED();
         }
         double t = 0.0;

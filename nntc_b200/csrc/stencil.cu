@@ -943,6 +943,7 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
     const int blocks = (int)(P.start[P.n] / ASM_THREADS);
     const size_t shared = (size_t)SLOTS * nmono * ASM_THREADS * sizeof(double);
     AsmArgs A{ d->weights, d->bias, d->cw, d->mono[level0], nmono };
+    NB_TRY(ktimer_begin(d, level0 ? NNTC_B200_K_ASSEMBLE0 : NNTC_B200_K_ASSEMBLE1));
     if (level0)
     {
         NB_CUDA(cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
@@ -953,6 +954,7 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
         NB_CUDA(cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
         k_assemble<false><<<blocks, ASM_THREADS, shared, d->stream>>>(P, A);
     }
+    NB_TRY(ktimer_end(d));
     NB_LAUNCHED();
     const Red R = red_for(d, P);
     const int tblocks = (int)(P.start[P.n] / THREADS);
@@ -1002,7 +1004,9 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     for (int it = 0; it < CG_MAX_IT; it++)
     {
         NB_CUDA(cudaMemsetAsync(active + (it % CG_PROBE), 0, sizeof(unsigned int), d->stream));
+        NB_TRY(ktimer_begin(d, NNTC_B200_K_MATVEC));
         k_cg_matvec<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+        NB_TRY(ktimer_end(d));
         NB_LAUNCHED();
         k_cg_alpha<<<P.n, 32, 0, d->stream>>>(P, R);
         NB_LAUNCHED();
@@ -1081,7 +1085,9 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
             if (C.start[C.n] == 0)
                 continue;
             SweepArgs A{ d->scalars, level0 ? d->lo0 : d->lo1, level0 ? d->hi0 : d->hi1, bits, cx, cy, d->counters + CNT_SWEEP };
+            NB_TRY(ktimer_begin(d, NNTC_B200_K_SWEEP));
             k_quant_sweep<<<(int)(C.start[C.n] / THREADS), THREADS, 0, d->stream>>>(C, A);
+            NB_TRY(ktimer_end(d));
             NB_LAUNCHED();
         }
     NB_CUDA(cudaEventRecord(d->ev[3], d->stream));
