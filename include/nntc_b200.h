@@ -268,6 +268,16 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
                                const double* per_site, nntc_b200_encode_result* r, uint8_t* const* k0,
                                uint8_t* const* k1, uint8_t* const* ep, uint8_t* const* sel);
 
+/* ---- kernel-shape options: the results are the same bits either way ---- */
+enum nntc_b200_option
+{
+    /* 1: assemble the stencils with one thread per texel recomputing every site it touches, the reference's shape
+     * (src/solve_level1.cu:259-581); 0 (default): one pass per site for the gradient terms, then one thread per
+     * (texel, slot) for the monomial sums. */
+    NNTC_B200_OPT_REFERENCE_SHAPED_ASSEMBLY = 0
+};
+int nntc_b200_set_option(nntc_b200_device* d, int option, int value);
+
 /* ---- measurement ---- */
 /* Kernels this library has launched since the process started (every launch, every device). */
 long long nntc_b200_launch_count(void);

@@ -79,6 +79,7 @@ PROTOTYPES = {
     "nntc_b200_encode_defaults": (None, [C.POINTER(abi.EncodeArgs)]),
     "nntc_b200_encode_on_device": (_I, [_P, _M, C.POINTER(abi.EncodeArgs), _PD, C.POINTER(abi.EncodeResult),
                                         _PPU8, _PPU8, _PPU8, _PPU8]),
+    "nntc_b200_set_option": (_I, [_P, _I, _I]),
     "nntc_b200_probe_normal_equations": (_I, [_P, _PD, _S]),
     "nntc_b200_probe_workspace": (_I, [_P, _I, _I, _PD, _PD, _PF, _PD, _PF]),
     "nntc_b200_probe_monomials": (_I, [_P, _I, _PD, _S]),

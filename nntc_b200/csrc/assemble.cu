@@ -1,0 +1,391 @@
+// assemble.cu: the stencil and gradient assembly of blocks (b) and (c'), restructured for B200 - and bit-identical
+// to the reference's per-texel gather (src/solve_level1.cu:259-581).
+//
+// The reference gives each texel one thread that walks every site whose bilinear footprint can reach it and, for each
+// site that does, recomputes the whole site: its G (or Q) matrix, its residual and G^T diag(cw) r - about a thousand
+// operations - then adds the site's monomials into five slots of fifteen sums. Every site is recomputed by each of the
+// (up to four) texels it touches, and the 75 double accumulators of a thread spill.
+//
+// Two observations make it cheap without changing a single rounding:
+//
+//   - the gradient term of a site, t_s = G^T diag(cw) r, does not depend on which texel gathers it. One thread per
+//     SITE computes it once, with the reference's arithmetic (rows in order, each column's sum over the rows in order,
+//     no contraction), into a per-site buffer of doubles; the gather then adds w_self * t_s exactly as the reference
+//     adds w_self * acc.
+//   - the stencil's monomial sums need only the site's sample of the OTHER latent (a bilinear blend of four texels) and
+//     the tap weights - a few dozen operations. They are gathered by one thread per (texel, slot): grid.y is the slot,
+//     so a warp shares one slot and its site range (the intersection of the two texels' footprints). Each slot's sums
+//     receive the same terms in the same site order as the reference's, so every sum, and the expansion against the
+//     monomial matrices after it, is the same bits.
+//
+// Every plane of the chain is in each launch (nb::Planes); the per-site buffer holds every plane's sites.
+
+#include <vector>
+
+#include "device.cuh"
+
+namespace nb
+{
+
+constexpr int SITE_THREADS = 256;
+constexpr int GATHER_THREADS = 128;
+
+// The ten products y_i y_k (i <= k < 4) of the monomial layout, row by row: (0,0) (0,1) (0,2) (0,3) (1,1) (1,2)
+// (1,3) (2,2) (2,3) (3,3). Functions rather than tables, so an unrolled index folds to a register name.
+__host__ __device__ constexpr int pair_i(int p)
+{
+    return p < 4 ? 0 : (p < 7 ? 1 : (p < 9 ? 2 : 3));
+}
+__host__ __device__ constexpr int pair_k(int p)
+{
+    return p < 4 ? p : (p < 7 ? p - 3 : (p < 9 ? p - 5 : 3));
+}
+
+struct SiteArgs
+{
+    const float* weights;
+    const float* bias;
+    const float* cw;
+    double* terms;                      // [site][c] over every plane
+    long long site0[MAX_PLANES + 1];    // the first site of each plane in `terms`
+};
+
+// One thread per site: t_s[a] = sum_r cw_r G[r][a] res_r (level 1, block b) or sum_r cw_r Q[r][a] res_r (level 0,
+// block c'), in the reference's order of operations (src/solve_level1.cu:335-361, 518-544).
+template <bool LEVEL0>
+__global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs A)
+{
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long si = base - P.start[pl] + threadIdx.x;
+    const int kc = P.kc, per = 1 + kc;
+    if (si >= (long long)V.w0 * V.h0 * per)
+        return;
+    const int c0 = P.c0, c1 = P.c1, nin = P.nin, nout = P.nout;
+    const long long pixel = si / per;
+    const int j = (int)(si % per);
+    const int px = (int)(pixel % V.w0), py = (int)(pixel / V.w0);
+    float dx, dy;
+    site_offset(kc, j, px, py, dx, dy);
+    float sbar[MAX_CH], cbar[MAX_CH];
+    const Tap tp = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
+    blend_u<MAX_CH>(V.v1, V.w1, c1, tp, cbar);
+    Tap t0{};
+    float w0[4];
+    if (j == 0)
+    {
+#pragma unroll
+        for (int i = 0; i < MAX_CH; i++)
+            if (i < c0)
+                sbar[i] = V.v0[pixel * c0 + i];
+    }
+    else
+    {
+        t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+        blend_u<MAX_CH>(V.v0, V.w0, c0, t0, sbar);
+        tap_weights(t0, w0);
+    }
+    double acc[MAX_CH];
+#pragma unroll
+    for (int a = 0; a < MAX_CH; a++)
+        acc[a] = 0.0;
+    for (int r = 0; r < nout; r++)
+    {
+        // the target of this output, sampled as blend() samples it
+        float target;
+        if (j == 0)
+            target = __ldg(V.src + pixel * nout + r);
+        else
+        {
+            const float* s = V.src + r;
+            target = w0[0] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x0) * nout) +
+                     w0[1] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x1) * nout) +
+                     w0[2] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x0) * nout) +
+                     w0[3] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x1) * nout);
+        }
+        const float* row = A.weights + (size_t)r * nin;
+        float out = A.bias[r];
+        float col[MAX_CH];
+        if (!LEVEL0)
+        {
+#pragma unroll
+            for (int i = 0; i < MAX_CH; i++)
+                if (i < c0)
+                    out += row[c1 + i] * sbar[i];
+#pragma unroll
+            for (int q = 0; q < MAX_CH; q++)
+                if (q < c1)
+                {
+                    float gg = row[q];
+#pragma unroll
+                    for (int i = 0; i < MAX_CH; i++)
+                        if (i < c0)
+                            gg += sbar[i] * row[c1 + c0 + i * c1 + q];
+                    col[q] = gg;
+                    out += gg * cbar[q];
+                }
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < MAX_CH; q++)
+                if (q < c1)
+                    out += row[q] * cbar[q];
+#pragma unroll
+            for (int i = 0; i < MAX_CH; i++)
+                if (i < c0)
+                {
+                    float qq = row[c1 + i];
+#pragma unroll
+                    for (int q = 0; q < MAX_CH; q++)
+                        if (q < c1)
+                            qq += cbar[q] * row[c1 + c0 + i * c1 + q];
+                    col[i] = qq;
+                    out += qq * sbar[i];
+                }
+        }
+        const float res = out - target;
+        const int c = LEVEL0 ? c0 : c1;
+#pragma unroll
+        for (int a = 0; a < MAX_CH; a++)
+            if (a < c)
+                acc[a] += (double)A.cw[r] * (double)col[a] * (double)res;
+    }
+    const int c = LEVEL0 ? c0 : c1;
+    double* out_t = A.terms + (size_t)(A.site0[pl] + si) * c;
+#pragma unroll
+    for (int a = 0; a < MAX_CH; a++)
+        if (a < c)
+            out_t[a] = acc[a];
+}
+
+// The pixels whose bilinear footprint into an n1-wide plane can reach texel ti (src/solve_level1.cu:246-257).
+__device__ __forceinline__ void reach(int ti, int n0, int n1, int& lo, int& hi)
+{
+    const double r = (double)n0 / (double)n1;
+    lo = (int)ceil(((double)ti - 0.5) * r - 1.0);
+    hi = (int)ceil(((double)ti + 1.5) * r) - 1;
+    lo = lo < 0 ? 0 : lo;
+    hi = hi > n0 - 1 ? n0 - 1 : hi;
+}
+
+struct GatherArgs
+{
+    const double* terms;
+    const double* mono;   // nmono matrices of c x c
+    int nmono;
+    long long site0[MAX_PLANES + 1];
+};
+
+// One thread per (texel, slot): the slot's monomial sums over every site that touches both the texel and the slot's
+// neighbour, in site order, expanded into the slot's block; the self-slot thread also gathers the gradient.
+template <bool LEVEL0>
+__global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs A)
+{
+    const int slot = blockIdx.y;
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long ti = base - P.start[pl] + threadIdx.x;
+    const int tw_ = V.w, th_ = V.h;
+    if (ti >= (long long)tw_ * th_)
+        return;
+    const int c0 = P.c0, c1 = P.c1, kc = P.kc, per = 1 + kc, nmono = A.nmono;
+    const int c = LEVEL0 ? c0 : c1;
+    const int tx = (int)(ti % tw_), ty = (int)(ti / tw_);
+    int ox, oy;
+    slot_offset(slot, ox, oy);
+    const int nbx = tx + ox, nby = ty + oy;
+    const size_t T = (size_t)tw_ * th_;
+    const int cc = c * c;
+    if (nbx < 0 || nbx >= tw_ || nby >= th_)
+    {
+        // no neighbour in this direction: the reference's block is zero (no site touches both)
+        for (int e = 0; e < cc; e++)
+            V.stencil[(size_t)(slot * cc + e) * T + ti] = 0.0;
+        return;
+    }
+    // the pixel range of sites that can touch both texels: the intersection of their footprints
+    int px_lo, px_hi, py_lo, py_hi, qx_lo, qx_hi, qy_lo, qy_hi;
+    const int n1x = LEVEL0 ? V.w0 : V.w1, n1y = LEVEL0 ? V.h0 : V.h1;
+    reach(tx, V.w0, n1x, px_lo, px_hi);
+    reach(ty, V.h0, n1y, py_lo, py_hi);
+    reach(nbx, V.w0, n1x, qx_lo, qx_hi);
+    reach(nby, V.h0, n1y, qy_lo, qy_hi);
+    px_lo = max(px_lo, qx_lo);
+    px_hi = min(px_hi, qx_hi);
+    py_lo = max(py_lo, qy_lo);
+    py_hi = min(py_hi, qy_hi);
+
+    double sums[MAX_MONO];
+#pragma unroll
+    for (int i = 0; i < MAX_MONO; i++)
+        sums[i] = 0.0;
+    double g[MAX_CH];
+#pragma unroll
+    for (int a = 0; a < MAX_CH; a++)
+        g[a] = 0.0;
+    const double* terms = A.terms + (size_t)A.site0[pl] * c;
+
+    for (int py = py_lo; py <= py_hi; py++)
+        for (int px = px_lo; px <= px_hi; px++)
+            for (int j = 0; j <= kc; j++)
+            {
+                float dx, dy;
+                site_offset(kc, j, px, py, dx, dy);
+                // The site's taps on the unknown latent. A merged tap's weight is the sum, in corner order, of the
+                // corner weights that landed on that texel (src/solve_level1.cu:287-316, 466-498): accumulating the
+                // corners of the self texel and of the neighbour from zero gives the same two weights.
+                float w_self = 0.0f, w_other = 0.0f;
+                bool has_self = false, has_other = false;
+                if (LEVEL0 && j == 0)
+                {
+                    has_self = px == tx && py == ty;
+                    has_other = px == nbx && py == nby;
+                    w_self = has_self ? 1.0f : 0.0f;
+                    w_other = has_other ? 1.0f : 0.0f;
+                }
+                else
+                {
+                    const Tap tq = LEVEL0 ? tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0)
+                                          : tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
+                    float cw4[4];
+                    tap_weights(tq, cw4);
+                    const int cx4[4] = { tq.x0, tq.x1, tq.x0, tq.x1 };
+                    const int cy4[4] = { tq.y0, tq.y0, tq.y1, tq.y1 };
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        if (cx4[q] == tx && cy4[q] == ty)
+                        {
+                            w_self += cw4[q];
+                            has_self = true;
+                        }
+                        if (cx4[q] == nbx && cy4[q] == nby)
+                        {
+                            w_other += cw4[q];
+                            has_other = true;
+                        }
+                    }
+                }
+                if (!has_self || !has_other)
+                    continue;
+                // the sample of the other latent at the site, and its monomials in a fixed layout: the constant,
+                // the four linear terms, then the ten products (i <= k) row by row; a narrower latent uses the
+                // entries whose indices are all below its channel count, which is the reference's order
+                float y[MAX_CH];
+                if (!LEVEL0)
+                {
+                    if (j == 0)
+                    {
+                        const size_t pi = (size_t)py * V.w0 + px;
+#pragma unroll
+                        for (int i = 0; i < MAX_CH; i++)
+                            if (i < c0)
+                                y[i] = __ldg(V.v0 + pi * c0 + i);
+                    }
+                    else
+                    {
+                        const Tap t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+                        blend_u<MAX_CH>(V.v0, V.w0, c0, t0, y);
+                    }
+                }
+                else
+                {
+                    const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
+                    blend_u<MAX_CH>(V.v1, V.w1, c1, t1, y);
+                }
+                const int ny_ = LEVEL0 ? c1 : c0;
+                if (slot == 0)
+                {
+                    const double* ts = terms + ((size_t)(py * V.w0 + px) * per + j) * c;
+#pragma unroll
+                    for (int a = 0; a < MAX_CH; a++)
+                        if (a < c)
+                            g[a] += (double)w_self * ts[a];
+                }
+                const double scale = (double)w_self * (double)w_other;
+                sums[0] += scale * 1.0;
+#pragma unroll
+                for (int i = 0; i < MAX_CH; i++)
+                    if (i < ny_)
+                        sums[1 + i] += scale * (double)y[i];
+#pragma unroll
+                for (int p = 0; p < 10; p++)
+                {
+                    const int i = pair_i(p), k2 = pair_k(p);
+                    if (k2 < ny_)
+                        sums[5 + p] += scale * ((double)y[i] * (double)y[k2]);
+                }
+            }
+
+    // the slot's block, expanded once against the monomial matrices in the reference's order (src/solve_level1.cu:382-399)
+    double blk[MAX_CH * MAX_CH];
+#pragma unroll
+    for (int e = 0; e < MAX_CH * MAX_CH; e++)
+        blk[e] = 0.0;
+    const int ny_ = LEVEL0 ? c1 : c0;
+    int q = 0;
+#pragma unroll
+    for (int L = 0; L < MAX_MONO; L++)
+    {
+        const bool valid = L == 0 || (L <= MAX_CH ? L - 1 < ny_ : pair_k(L - 5) < ny_);
+        if (!valid)
+            continue;
+        const double s = sums[L];
+        const double* mat = A.mono + (size_t)q * cc;
+        q++;
+        if (s == 0.0)
+            continue;
+#pragma unroll
+        for (int e = 0; e < MAX_CH * MAX_CH; e++)
+            if (e < cc)
+                blk[e] += s * __ldg(mat + e);
+    }
+#pragma unroll
+    for (int e = 0; e < MAX_CH * MAX_CH; e++)
+        if (e < cc)
+            V.stencil[(size_t)(slot * cc + e) * T + ti] = blk[e];
+    if (slot == 0)
+    {
+#pragma unroll
+        for (int a = 0; a < MAX_CH; a++)
+            if (a < c)
+                V.grad[ti * c + a] = g[a];
+    }
+}
+
+// Launch both passes for every plane: the per-site terms, then the per-(texel, slot) gather.
+int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono)
+{
+    Planes S = planes_for(d, level0, [&](int i) {
+        const DevPlane& p = d->planes[(size_t)i];
+        return (size_t)p.w0 * p.h0 * (size_t)(1 + k);
+    });
+    S.kc = k;
+    SiteArgs A{ d->weights, d->bias, d->cw, d->site_terms, {} };
+    GatherArgs G{ d->site_terms, d->mono[level0], nmono, {} };
+    long long at = 0;
+    for (int i = 0; i < S.n; i++)
+    {
+        A.site0[i] = G.site0[i] = at;
+        at += (long long)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0 * (1 + k);
+    }
+    A.site0[S.n] = G.site0[S.n] = at;
+    const int sblocks = (int)(S.start[S.n] / SITE_THREADS);
+    if (level0)
+        k_site_terms<true><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A);
+    else
+        k_site_terms<false><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A);
+    NB_LAUNCHED();
+    dim3 grid((unsigned)(P_texels.start[P_texels.n] / GATHER_THREADS), SLOTS);
+    if (level0)
+        k_gather<true><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+    else
+        k_gather<false><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+    NB_LAUNCHED();
+    return NNTC_B200_OK;
+}
+
+}   // namespace nb

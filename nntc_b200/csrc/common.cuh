@@ -122,6 +122,22 @@ __host__ __device__ __forceinline__ void blend(const float* plane, int w, int c,
         out[k] = wt[0] * a[k] + wt[1] * b[k] + wt[2] * e[k] + wt[3] * f[k];
 }
 
+// blend() with the channel loop unrolled to MAXC and guarded, so `out` stays in registers; the same arithmetic.
+template <int MAXC>
+__device__ __forceinline__ void blend_u(const float* plane, int w, int c, const Tap& t, float* out)
+{
+    const float* a = plane + ((size_t)t.y0 * w + t.x0) * c;
+    const float* b = plane + ((size_t)t.y0 * w + t.x1) * c;
+    const float* e = plane + ((size_t)t.y1 * w + t.x0) * c;
+    const float* f = plane + ((size_t)t.y1 * w + t.x1) * c;
+    float wt[4];
+    tap_weights(t, wt);
+#pragma unroll
+    for (int k = 0; k < MAXC; k++)
+        if (k < c)
+            out[k] = wt[0] * __ldg(a + k) + wt[1] * __ldg(b + k) + wt[2] * __ldg(e + k) + wt[3] * __ldg(f + k);
+}
+
 // phi in the shader's order: [c_j] [s_i] [s_i c_j], i outer (src/sample.cuh:74-85).
 template <typename T>
 __host__ __device__ __forceinline__ int features(const T* s, int c0, const T* c, int c1, T* phi)

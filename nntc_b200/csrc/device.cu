@@ -551,6 +551,15 @@ int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain,
     NB_CK(cudaMemset(d->reduction, 0, entries * sizeof(double)));
     NB_ALLOC(d->bc_stats, (size_t)MAX_PLANES * 2 * sizeof(double));
     {
+        // The assembly's per-site gradient terms: every site of every plane at the largest K (4), one double per channel
+        // of the wider unknown.
+        size_t sites = 0;
+        for (const DevPlane& p : d->planes)
+            sites += (size_t)p.w0 * p.h0 * 5;
+        d->site_terms_count = sites * (size_t)std::max(m->c0, m->c1);
+        NB_ALLOC(d->site_terms, d->site_terms_count * sizeof(double));
+    }
+    {
         // The objective's partials: one triple per 256-pixel block of every plane, then the three sums per plane.
         size_t blocks = 0;
         for (const DevPlane& p : d->planes)
@@ -604,7 +613,7 @@ void nntc_b200_device_destroy(nntc_b200_device* d)
     }
     void* bufs[] = { d->weights, d->bias,     d->palette,   d->lo1,      d->hi1,         d->lo0,
                      d->hi0,     d->cw,       d->mono[0],   d->mono[1],  d->partial,     d->scalars,
-                     d->counters, d->reduction, d->ls_partial, d->obj_partial, d->bc_stats, d->resid,
+                     d->counters, d->reduction, d->ls_partial, d->obj_partial, d->bc_stats, d->resid, d->site_terms,
                      d->means,   d->cov,      d->hist,      d->scratch,  d->scratch8,    d->rgb8 };
     for (void* b : bufs)
         cudaFree(b);

@@ -928,6 +928,8 @@ static Red red_for(nntc_b200_device* d, const Planes& P)
     return Red{ d->partial, (size_t)(P.start[P.n] / THREADS), d->scalars };
 }
 
+int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono);
+
 int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0)
 {
     if (level0 && !d->l0_bc8)
@@ -944,7 +946,9 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
     const size_t shared = (size_t)SLOTS * nmono * ASM_THREADS * sizeof(double);
     AsmArgs A{ d->weights, d->bias, d->cw, d->mono[level0], nmono };
     NB_TRY(ktimer_begin(d, level0 ? NNTC_B200_K_ASSEMBLE0 : NNTC_B200_K_ASSEMBLE1));
-    if (level0)
+    if (!d->reference_shaped_assembly && k <= 4)
+        NB_TRY(assemble_split(d, k, level0, P, nmono));
+    else if (level0)
     {
         NB_CUDA(cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
         k_assemble<true><<<blocks, ASM_THREADS, shared, d->stream>>>(P, A);
@@ -955,7 +959,8 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
         k_assemble<false><<<blocks, ASM_THREADS, shared, d->stream>>>(P, A);
     }
     NB_TRY(ktimer_end(d));
-    NB_LAUNCHED();
+    if (d->reference_shaped_assembly || k > 4)
+        NB_LAUNCHED();
     const Red R = red_for(d, P);
     const int tblocks = (int)(P.start[P.n] / THREADS);
     k_diag<<<tblocks, THREADS, 0, d->stream>>>(P, R);
@@ -1137,6 +1142,17 @@ using namespace nb;
 
 extern "C"
 {
+
+int nntc_b200_set_option(nntc_b200_device* d, int option, int value)
+{
+    if (option == NNTC_B200_OPT_REFERENCE_SHAPED_ASSEMBLY)
+    {
+        d->reference_shaped_assembly = value != 0;
+        return NNTC_B200_OK;
+    }
+    set_error(NNTC_B200_ERR_ARG, "no such option");
+    return NNTC_B200_ERR_ARG;
+}
 
 int nntc_b200_solve_level1_all(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
                                nntc_b200_plane_report* rep, double* ms)

@@ -231,3 +231,25 @@ def test_bc_refine_vs_oracle(textures, c0, c1, w, h):
                                                     O.fptr(v), O.u8ptr(kk), C.byref(imp))
             assert np.array_equal(geps[i], eps[i]) and np.array_equal(gsels[i], sels[i]), f"plane {i}"
             assert np.array_equal(s.get_v0(i), v)
+
+
+@pytest.mark.parametrize("textures,c0,c1,w,h", [(4, 4, 4, 72, 40), (1, 3, 2, 45, 29)])
+def test_assembly_shapes_agree_bit_for_bit(textures, c0, c1, w, h):
+    """The per-site + per-(texel, slot) assembly and the reference-shaped per-texel gather give the same bits."""
+    from nntc_b200 import lib
+    mat = materials.small(41 + w, w, h, textures=textures, c0=c0, c1=c1)
+    dw, db, v0, v1 = random_state(mat, 3 * w + h)
+    out = []
+    for shaped in (0, 1):
+        with Session(mat) as s:
+            assert lib().nntc_b200_set_option(s.d, 0, shaped) == 0
+            for i in range(len(mat.planes)):
+                s.set_planes(i, v0[i], v1[i])
+            s.set_decoder(dw, db)
+            s.set_grids(np.full(c0, -1.0), np.full(c0, 1.0))
+            s.block(False)
+            s.block(True)
+            out.append([(s.workspace(i, False), s.workspace(i, True)) for i in range(len(mat.planes))])
+    for (a1, a0), (b1, b0) in zip(*out):
+        for key in ("stencil", "grad", "x"):
+            assert np.array_equal(a1[key], b1[key]) and np.array_equal(a0[key], b0[key]), key
