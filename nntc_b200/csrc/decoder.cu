@@ -94,19 +94,18 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape 
     const bool worker = kg < S.ks;
     const int r0 = S.trow[tile] * TILE, cc0 = S.tcol[tile] * TILE;   // row in [V|T] column space, col in V
     double acc[TILE][TILE];
+#pragma unroll
     for (int a = 0; a < TILE; a++)
+#pragma unroll
         for (int b = 0; b < TILE; b++)
             acc[a][b] = 0.0;
 
     for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
     {
         const size_t si = chunk * LS_THREADS + tid;
-        float phi[MAX_NIN], tgt[MAX_NOUT];
-        float one = 0.0f;
-        for (int i = 0; i < nin; i++)
-            phi[i] = 0.0f;
-        for (int c = 0; c < nout; c++)
-            tgt[c] = 0.0f;
+        __syncthreads();   // the previous chunk's tiles have finished reading
+        // The site's row [phi | 1 | t] staged straight into shared memory, each value with the solver's arithmetic
+        // (src/sample.cuh:154-178); a site outside the plane stages a row of zeros.
         if (si < sites)
         {
             const size_t pixel = si / (size_t)per_pixel;
@@ -116,33 +115,62 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape 
             site_offset(kc, j, px, py, dx, dy);
             float s[MAX_CH], c[MAX_CH];
             const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
-            blend<MAX_CH>(V.v1, V.w1, c1, t1, c);
+            blend_u<MAX_CH>(V.v1, V.w1, c1, t1, c);
+            Tap t0{};
+            float w4[4];
             if (j == 0)
             {
-                for (int i = 0; i < c0; i++)
-                    s[i] = V.v0[pixel * c0 + i];
-                for (int i = 0; i < nout; i++)
-                    tgt[i] = __ldg(V.src + pixel * nout + i);
+#pragma unroll
+                for (int i = 0; i < MAX_CH; i++)
+                    if (i < c0)
+                        s[i] = __ldg(V.v0 + pixel * c0 + i);
             }
             else
             {
-                const Tap t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
-                blend<MAX_CH>(V.v0, V.w0, c0, t0, s);
-                blend<MAX_NOUT>(V.src, V.w0, nout, t0, tgt);
+                t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+                blend_u<MAX_CH>(V.v0, V.w0, c0, t0, s);
+                tap_weights(t0, w4);
             }
-            features(s, c0, c, c1, phi);
-            one = 1.0f;
+            int q = 0;
+#pragma unroll
+            for (int jj = 0; jj < MAX_CH; jj++)
+                if (jj < c1)
+                    sx[(q++) * LS_STRIDE + tid] = c[jj];
+#pragma unroll
+            for (int i = 0; i < MAX_CH; i++)
+                if (i < c0)
+                    sx[(q++) * LS_STRIDE + tid] = s[i];
+#pragma unroll
+            for (int i = 0; i < MAX_CH; i++)
+#pragma unroll
+                for (int jj = 0; jj < MAX_CH; jj++)
+                    if (i < c0 && jj < c1)
+                        sx[(q++) * LS_STRIDE + tid] = s[i] * c[jj];
+            sx[nin * LS_STRIDE + tid] = 1.0f;
+            for (int r = 0; r < nout; r++)
+            {
+                float t;
+                if (j == 0)
+                    t = __ldg(V.src + pixel * nout + r);
+                else
+                    t = w4[0] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x0) * nout + r) +
+                        w4[1] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x1) * nout + r) +
+                        w4[2] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x0) * nout + r) +
+                        w4[3] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x1) * nout + r);
+                sx[(VP + r) * LS_STRIDE + tid] = t;
+            }
         }
-        __syncthreads();   // the previous chunk's tiles have finished reading
-        for (int i = 0; i < nin; i++)
-            sx[i * LS_STRIDE + tid] = phi[i];
-        sx[nin * LS_STRIDE + tid] = one;
+        else
+        {
+            for (int i = 0; i < mm; i++)
+                sx[i * LS_STRIDE + tid] = 0.0f;
+            for (int r = 0; r < nout; r++)
+                sx[(VP + r) * LS_STRIDE + tid] = 0.0f;
+        }
         for (int i = mm; i < VP; i++)
             sx[i * LS_STRIDE + tid] = 0.0f;
-        for (int c = 0; c < nout; c++)
-            sx[(VP + c) * LS_STRIDE + tid] = tgt[c];
-        for (int c = nout; c < TP; c++)
-            sx[(VP + c) * LS_STRIDE + tid] = 0.0f;
+        for (int r = nout; r < TP; r++)
+            sx[(VP + r) * LS_STRIDE + tid] = 0.0f;
         __syncthreads();
         if (worker)
         {
@@ -151,12 +179,15 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape 
             for (int p = kg; p < LS_THREADS; p += S.ks)
             {
                 double a[TILE], b[TILE];
+#pragma unroll
                 for (int q = 0; q < TILE; q++)
                 {
                     a[q] = (double)rowp[q * LS_STRIDE + p];
                     b[q] = (double)colp[q * LS_STRIDE + p];
                 }
+#pragma unroll
                 for (int x = 0; x < TILE; x++)
+#pragma unroll
                     for (int y = 0; y < TILE; y++)
                         acc[x][y] = fma(a[x], b[y], acc[x][y]);
             }
@@ -164,7 +195,9 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape 
     }
 
     // Fold the k-slices in order 0..ks-1, entry by entry, and write the entries this tile owns.
+#pragma unroll
     for (int x = 0; x < TILE; x++)
+#pragma unroll
         for (int y = 0; y < TILE; y++)
         {
             __syncthreads();

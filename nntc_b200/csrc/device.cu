@@ -550,6 +550,7 @@ int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain,
     NB_ALLOC(d->reduction, entries * sizeof(double));
     NB_CK(cudaMemset(d->reduction, 0, entries * sizeof(double)));
     NB_ALLOC(d->bc_stats, (size_t)MAX_PLANES * 2 * sizeof(double));
+    NB_ALLOC(d->radix, (size_t)std::max(2 * MAX_CH * 2048, MAX_NOUT * MAX_NOUT) * sizeof(unsigned int));
     {
         // The assembly's per-site gradient terms: every site of every plane at the largest K (4), one double per channel
         // of the wider unknown.
@@ -614,6 +615,7 @@ void nntc_b200_device_destroy(nntc_b200_device* d)
     void* bufs[] = { d->weights, d->bias,     d->palette,   d->lo1,      d->hi1,         d->lo0,
                      d->hi0,     d->cw,       d->mono[0],   d->mono[1],  d->partial,     d->scalars,
                      d->counters, d->reduction, d->ls_partial, d->obj_partial, d->bc_stats, d->resid, d->site_terms,
+                     d->radix,
                      d->means,   d->cov,      d->hist,      d->scratch,  d->scratch8,    d->rgb8 };
     for (void* b : bufs)
         cudaFree(b);

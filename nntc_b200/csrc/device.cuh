@@ -106,6 +106,7 @@ struct nntc_b200_device
     double* ls_partial = nullptr;        // entries * LS_GRID
     double* obj_partial = nullptr;       // 3 * MAX_PLANES * OBJ_GRID
     double* bc_stats = nullptr;          // MAX_PLANES * 2
+    unsigned int* radix = nullptr;       // 2 * MAX_CH * 2048 words: the grid fit's histograms and flags
     double* site_terms = nullptr;        // every site's gradient term of the assembly, max(C0, C1) per site at K = 4
     size_t site_terms_count = 0;         // doubles in site_terms
     int reference_shaped_assembly = 0;   // 1: the per-texel gather of the reference's shape (same bits, slower)

@@ -23,24 +23,63 @@ namespace
 
 constexpr double E_REL = 1e-6, E_NOISE = 1e-8;   // src/main.cpp:371-372 (the rise warning, not a decision)
 
-struct Planes8
+// Both latents' planes, indices and BC state of every plane, copied device to device: what the outer repack loop
+// restores when a pass does not lower the shipped E.
+struct DeviceCopy
 {
-    std::vector<std::vector<uint8_t>> buf;
-    std::vector<uint8_t*> ptr;
-    void size(const nntc_b200_model& m, int level, int c)
+    void* buf = nullptr;
+    size_t bytes = 0;
+    ~DeviceCopy()
     {
-        buf.assign((size_t)m.nplanes, std::vector<uint8_t>());
-        ptr.assign((size_t)m.nplanes, nullptr);
-        for (int i = 0; i < m.nplanes; i++)
-        {
-            const size_t n = level == 0 ? (size_t)m.w0[i] * m.h0[i] * c : (size_t)m.w1[i] * m.h1[i] * c;
-            buf[(size_t)i].assign(n, 0);
-            ptr[(size_t)i] = buf[(size_t)i].data();
-        }
+        if (buf)
+            cudaFree(buf);
     }
 };
 
+int snapshot(nntc_b200_device* d, DeviceCopy& keep, bool save)
+{
+    std::vector<std::pair<void*, size_t>> parts;
+    for (nb::DevPlane& p : d->planes)
+    {
+        const size_t n0 = (size_t)p.w0 * p.h0 * d->c0, n1 = (size_t)p.w1 * p.h1 * d->c1;
+        parts.push_back({ p.v0, n0 * sizeof(float) });
+        parts.push_back({ p.k0, n0 });
+        parts.push_back({ p.v1, n1 * sizeof(float) });
+        parts.push_back({ p.k1, n1 });
+        if (p.bc_ep)
+        {
+            parts.push_back({ p.bc_ep, p.blocks() * d->c0 * 2 });
+            parts.push_back({ p.bc_sel, p.blocks() * d->c0 * 16 });
+        }
+    }
+    size_t total = 0;
+    for (auto& q : parts)
+        total += (q.second + 255) / 256 * 256;
+    if (!keep.buf)
+    {
+        NB_CUDA(cudaMalloc(&keep.buf, total));
+        keep.bytes = total;
+    }
+    size_t at = 0;
+    for (auto& q : parts)
+    {
+        char* slot = (char*)keep.buf + at;
+        if (save)
+            NB_CUDA(cudaMemcpyAsync(slot, q.first, q.second, cudaMemcpyDeviceToDevice, d->stream));
+        else
+            NB_CUDA(cudaMemcpyAsync(q.first, slot, q.second, cudaMemcpyDeviceToDevice, d->stream));
+        at += (q.second + 255) / 256 * 256;
+    }
+    NB_CUDA(cudaStreamSynchronize(d->stream));
+    return NNTC_B200_OK;
+}
+
 }   // namespace
+
+namespace nb
+{
+int channel_copies(nntc_b200_device* d, std::vector<unsigned char>& same);
+}
 
 using namespace nb;
 
@@ -98,9 +137,6 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     }
     m->has_lo1 = 0;
 
-    Planes8 k0, k1;
-    k0.size(*m, 0, m->c0);
-    k1.size(*m, 1, m->c1);
     nntc_b200_objective e{};
     double ms = 0.0;
     auto objective = [&](nntc_b200_objective& out) {
@@ -116,33 +152,23 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     };
 
     // ---- initialisation (src/main.cpp:1930-2122)
-    NB_TRY(nntc_b200_init_level0(d, m, a->luma, m->init0_residual ? 0 : 1, k0.ptr.data()));
+    NB_TRY(nntc_b200_init_level0(d, m, a->luma, m->init0_residual ? 0 : 1, nullptr));
     nntc_b200_init1_report irep{};
-    NB_TRY(nntc_b200_init_level1(d, m, a->init_pca, &irep, k1.ptr.data()));
+    NB_TRY(nntc_b200_init_level1(d, m, a->init_pca, &irep, nullptr));
     if (!a->init_pca)
     {
         // The box init takes the source channels in order with every exact copy of an earlier channel moved to the
         // back (src/main.cpp:1938-2012); where that changes which channels are taken, level 1 is re-formed from them.
         const int nout = m->nout, taken = m->c1 < nout ? m->c1 : nout;
-        std::vector<std::vector<float>> src((size_t)np);
-        for (int i = 0; i < np; i++)
-        {
-            src[(size_t)i].resize((size_t)m->w0[i] * m->h0[i] * nout);
-            NB_TRY(download(d, src[(size_t)i].data(), d->planes[(size_t)i].src, src[(size_t)i].size() * sizeof(float)));
-        }
+        std::vector<unsigned char> same;
+        NB_TRY(channel_copies(d, same));
         std::vector<int> order, copies;
-        for (int s = 0; s < nout; s++)
+        for (int s2 = 0; s2 < nout; s2++)
         {
             bool copy = false;
-            for (int e2 = 0; e2 < s && !copy; e2++)
-            {
-                bool same = true;
-                for (int i = 0; i < np && same; i++)
-                    for (size_t t = 0; t < src[(size_t)i].size() / (size_t)nout && same; t++)
-                        same = src[(size_t)i][t * nout + s] == src[(size_t)i][t * nout + e2];
-                copy = same;
-            }
-            (copy ? copies : order).push_back(s);
+            for (int e2 = 0; e2 < s2 && !copy; e2++)
+                copy = same[(size_t)s2 * nout + e2] != 0;
+            (copy ? copies : order).push_back(s2);
         }
         order.insert(order.end(), copies.begin(), copies.end());
         std::vector<int> chosen(order.begin(), order.begin() + taken);
@@ -152,6 +178,13 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             plain = plain && chosen[(size_t)c] == c;
         if (!plain)
         {
+            std::vector<std::vector<float>> src((size_t)np);
+            for (int i = 0; i < np; i++)
+            {
+                src[(size_t)i].resize((size_t)m->w0[i] * m->h0[i] * nout);
+                NB_TRY(download(d, src[(size_t)i].data(), d->planes[(size_t)i].src,
+                                src[(size_t)i].size() * sizeof(float)));
+            }
             for (int i = 0; i < np; i++)
             {
                 const int w0 = m->w0[i], h0 = m->h0[i], w1 = m->w1[i], h1 = m->h1[i];
@@ -186,7 +219,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
                     }
                 NB_TRY(nntc_b200_level1_upload(d, i, v1.data(), v1.size()));
             }
-            NB_TRY(nntc_b200_quantise_level1(d, m, 0, k1.ptr.data()));
+            NB_TRY(nntc_b200_quantise_level1(d, m, 0, nullptr));
         }
     }
     NB_TRY(objective(e));
@@ -197,7 +230,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
         for (int c = 0; c < m->c0; c++)
         {
             nntc_b200_init0_report crep{};
-            NB_TRY(nntc_b200_init0_residual_channel(d, m, c, per_site, &crep, k0.ptr.data()));
+            NB_TRY(nntc_b200_init0_residual_channel(d, m, c, per_site, &crep, nullptr));
             NB_TRY(objective(e));
             NB_TRY(block_a());
             NB_TRY(objective(e));
@@ -223,9 +256,9 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
         NB_TRY(objective(ea));
         if (a->q1_start > 0 && round >= a->q1_start && !frozen)
         {
-            NB_TRY(nntc_b200_freeze_level1_grid(d, m, a->range_pct, k1.ptr.data()));
+            NB_TRY(nntc_b200_freeze_level1_grid(d, m, a->range_pct, nullptr));
             if (bc8)
-                NB_TRY(nntc_b200_freeze_level0_grid(d, m, a->range_pct, k0.ptr.data()));
+                NB_TRY(nntc_b200_freeze_level0_grid(d, m, a->range_pct, nullptr));
             frozen = true;
         }
         if (frozen)
@@ -283,7 +316,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     if (frozen)
         NB_TRY(nntc_b200_sweep_level1_all(d, m, k, a->ridge, a->q1_sweeps, lr.data(), &ms));
     else
-        NB_TRY(nntc_b200_quantise_level1(d, m, a->range_pct, k1.ptr.data()));
+        NB_TRY(nntc_b200_quantise_level1(d, m, a->range_pct, nullptr));
     r->ms_b += frozen ? ms : 0.0;
     if (bc8)
     {
@@ -293,7 +326,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             r->ms_c += ms;
         }
         else
-            NB_TRY(nntc_b200_quantise_level0(d, m, a->range_pct, k0.ptr.data()));
+            NB_TRY(nntc_b200_quantise_level0(d, m, a->range_pct, nullptr));
     }
     else
     {
@@ -302,8 +335,6 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
         r->ms_c += ms;
     }
     NB_TRY(block_a());
-    for (int i = 0; i < np; i++)
-        NB_TRY(nntc_b200_level0_download(d, i, k0.ptr[(size_t)i], k0.buf[(size_t)i].size()));
     NB_TRY(objective(e));
     r->e_after_rounds = e.e;
 
@@ -316,7 +347,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             return st;
         };
         nntc_b200_objective probe{};
-        NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, (const uint8_t* const*)k0.ptr.data(), &ms));
+        NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, nullptr, &ms));
         r->ms_pack += ms;
         std::vector<nntc_b200_bc_report> rp((size_t)(a->bc_refine > 0 ? a->bc_refine : 1));
         NB_TRY(nntc_b200_bc_refine(d, m, a->bc_refine, rp.data(), &ms));
@@ -334,33 +365,12 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             NB_TRY(objective(probe));
         }
         double e_ship = probe.e;
+        DeviceCopy keep;
         for (int pass = 1; pass <= a->bc_outer; pass++)
         {
-            // Everything a rejected pass would leave behind, kept (src/main.cpp:2561-2590).
-            std::vector<std::vector<float>> keep_v0((size_t)np), keep_v1((size_t)np);
-            std::vector<std::vector<uint8_t>> keep_k0((size_t)np), keep_k1((size_t)np), keep_ep((size_t)np),
-                keep_sel((size_t)np);
-            std::vector<uint8_t*> pe((size_t)np), ps((size_t)np);
-            for (int i = 0; i < np; i++)
-            {
-                const DevPlane& p = d->planes[(size_t)i];
-                keep_v0[(size_t)i].resize((size_t)p.w0 * p.h0 * m->c0);
-                keep_v1[(size_t)i].resize((size_t)p.w1 * p.h1 * m->c1);
-                keep_k0[(size_t)i].resize(keep_v0[(size_t)i].size());
-                keep_k1[(size_t)i].resize(keep_v1[(size_t)i].size());
-                keep_ep[(size_t)i].resize(p.blocks() * m->c0 * 2);
-                keep_sel[(size_t)i].resize(p.blocks() * m->c0 * 16);
-                pe[(size_t)i] = keep_ep[(size_t)i].data();
-                ps[(size_t)i] = keep_sel[(size_t)i].data();
-                NB_TRY(nntc_b200_level0_download_values(d, i, keep_v0[(size_t)i].data(), keep_v0[(size_t)i].size()));
-                NB_TRY(nntc_b200_level0_download(d, i, keep_k0[(size_t)i].data(), keep_k0[(size_t)i].size()));
-                NB_TRY(nntc_b200_level1_download(d, i, keep_v1[(size_t)i].data(), keep_v1[(size_t)i].size()));
-                NB_TRY(nntc_b200_level1_download_indices(d, i, keep_k1[(size_t)i].data(), keep_k1[(size_t)i].size()));
-            }
-            NB_TRY(nntc_b200_bc_state_save(d, m, pe.data(), ps.data()));
+            // Everything a rejected pass would leave behind, kept on the device (src/main.cpp:2561-2590).
+            NB_TRY(snapshot(d, keep, true));
             const nntc_b200_model keep_m = *m;
-            const Planes8 keep_mk0 = k0, keep_mk1 = k1;
-
             NB_TRY(refit_level1());
             NB_TRY(block_a());
             if (frozen)
@@ -368,12 +378,10 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             else
             {
                 NB_TRY(nntc_b200_solve_level0_cont_all(d, m, k, a->ridge, lr0.data(), &ms));
-                NB_TRY(nntc_b200_snap_level0_on_grid(d, m, k0.ptr.data()));
+                NB_TRY(nntc_b200_snap_level0_on_grid(d, m, nullptr));
             }
             r->ms_c += ms;
-            for (int i = 0; i < np; i++)
-                NB_TRY(nntc_b200_level0_download(d, i, k0.ptr[(size_t)i], k0.buf[(size_t)i].size()));
-            NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, (const uint8_t* const*)k0.ptr.data(), &ms));
+            NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, nullptr, &ms));
             r->ms_pack += ms;
             NB_TRY(nntc_b200_bc_refine(d, m, a->bc_refine, rp.data(), &ms));
             r->ms_refine += ms;
@@ -384,21 +392,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
                 r->outer_taken++;
                 continue;
             }
-            for (int i = 0; i < np; i++)
-            {
-                NB_TRY(nntc_b200_level0_upload(d, i, keep_v0[(size_t)i].data(), keep_v0[(size_t)i].size()));
-                NB_TRY(nntc_b200_level0_upload_indices(d, i, keep_k0[(size_t)i].data(), keep_k0[(size_t)i].size()));
-                NB_TRY(nntc_b200_level1_upload(d, i, keep_v1[(size_t)i].data(), keep_v1[(size_t)i].size()));
-                NB_TRY(nntc_b200_level1_upload_indices(d, i, keep_k1[(size_t)i].data(), keep_k1[(size_t)i].size()));
-            }
-            k0 = keep_mk0;
-            k1 = keep_mk1;
-            for (int i = 0; i < np; i++)
-            {
-                k0.ptr[(size_t)i] = k0.buf[(size_t)i].data();
-                k1.ptr[(size_t)i] = k1.buf[(size_t)i].data();
-            }
-            NB_TRY(nntc_b200_bc_state_restore(d, m, (const uint8_t* const*)pe.data(), (const uint8_t* const*)ps.data()));
+            NB_TRY(snapshot(d, keep, false));
             *m = keep_m;
             NB_TRY(nntc_b200_upload_decoder(d, m));
             NB_TRY(nntc_b200_upload_grids(d, m));

@@ -361,14 +361,21 @@ static int cov_sums(nntc_b200_device* d, const float* rows, size_t count, int no
     return NNTC_B200_OK;
 }
 
+int fit_grid_device(nntc_b200_device* d, int level0, bool pct, float* lo, float* hi);
+
+// Fit the grid (when `fit`) and snap every plane onto it. With `cont` empty both read the planes where the device holds
+// them; with a host copy (the pca init's projections) the fit is the host's and the snap reads the copy.
 static int fit_and_snap(nntc_b200_device* d, nntc_b200_model* m, int level0,
                         const std::vector<std::vector<float>>& cont, bool pct, uint8_t* const* k_out, bool fit)
 {
     const int nc = level0 ? d->c0 : d->c1;
     if (fit)
     {
-        std::vector<float> lo, hi;
-        fit_range(cont, nc, pct, lo, hi);
+        std::vector<float> lo(MAX_CH), hi(MAX_CH);
+        if (cont.empty())
+            NB_TRY(fit_grid_device(d, level0, pct, lo.data(), hi.data()));   // the planes as the device holds them
+        else
+            fit_range(cont, nc, pct, lo, hi);
         for (int c = 0; c < nc; c++)
             if (!(hi[(size_t)c] > lo[(size_t)c]))
             {
@@ -413,19 +420,6 @@ static int fit_and_snap(nntc_b200_device* d, nntc_b200_model* m, int level0,
             NB_TRY(download(d, k_out[i], k, n));
     }
     NB_CUDA(cudaStreamSynchronize(d->stream));
-    return NNTC_B200_OK;
-}
-
-static int download_planes(nntc_b200_device* d, int level0, std::vector<std::vector<float>>& cont)
-{
-    cont.assign(d->planes.size(), std::vector<float>());
-    for (size_t i = 0; i < d->planes.size(); i++)
-    {
-        const DevPlane& p = d->planes[i];
-        const size_t n = level0 ? (size_t)p.w0 * p.h0 * d->c0 : (size_t)p.w1 * p.h1 * d->c1;
-        cont[i].resize(n);
-        NB_TRY(download(d, cont[i].data(), level0 ? p.v0 : p.v1, n * sizeof(float)));
-    }
     return NNTC_B200_OK;
 }
 
@@ -494,13 +488,11 @@ int nntc_b200_init_level1(nntc_b200_device* d, nntc_b200_model* m, int pca, nntc
         {
             const DevPlane& p = d->planes[i];
             const size_t n = (size_t)p.w1 * p.h1;
-            k_init_level1_box<<<grid_for(n, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, nout, p.w1, p.h1, c1,
-                                                                       d->scratch);
+            k_init_level1_box<<<grid_for(n, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, nout, p.w1, p.h1, c1, p.v1);
             NB_LAUNCHED();
-            cont[i].resize(n * c1);
-            NB_TRY(download(d, cont[i].data(), d->scratch, n * c1 * sizeof(float)));
         }
-        return fit_and_snap(d, m, 0, cont, false, k1_out, true);
+        const std::vector<std::vector<float>> on_device;
+        return fit_and_snap(d, m, 0, on_device, false, k1_out, true);
     }
     // The basis: the base plane's block means, their covariance, the host eigenproblem.
     std::vector<double> raw;
@@ -743,16 +735,14 @@ int nntc_b200_init0_residual_channel(nntc_b200_device* d, const nntc_b200_model*
 
 int nntc_b200_quantise_level1(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k1_out)
 {
-    std::vector<std::vector<float>> cont;
-    NB_TRY(download_planes(d, 0, cont));
-    return fit_and_snap(d, m, 0, cont, range_pct != 0, k1_out, true);
+    const std::vector<std::vector<float>> on_device;
+    return fit_and_snap(d, m, 0, on_device, range_pct != 0, k1_out, true);
 }
 
 int nntc_b200_freeze_level1_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k1_out)
 {
-    std::vector<std::vector<float>> cont;
-    NB_TRY(download_planes(d, 0, cont));
-    return fit_and_snap(d, m, 0, cont, range_pct != 0, k1_out, true);
+    const std::vector<std::vector<float>> on_device;
+    return fit_and_snap(d, m, 0, on_device, range_pct != 0, k1_out, true);
 }
 
 static int level0_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out)
@@ -762,9 +752,8 @@ static int level0_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, u
         set_error(NNTC_B200_ERR_STATE, "level 0 has a grid only under --l0 bc8");
         return NNTC_B200_ERR_STATE;
     }
-    std::vector<std::vector<float>> cont;
-    NB_TRY(download_planes(d, 1, cont));
-    return fit_and_snap(d, m, 1, cont, range_pct != 0, k0_out, true);
+    const std::vector<std::vector<float>> on_device;
+    return fit_and_snap(d, m, 1, on_device, range_pct != 0, k0_out, true);
 }
 
 int nntc_b200_quantise_level0(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out)

@@ -28,6 +28,9 @@ struct ObjArgs
     double* partial;   // [3][total blocks]
 };
 
+// The bilinear rule in double at u, v (src/objective.cu:97-118), the channel loop unrolled to MAXC and guarded so
+// the result stays in registers.
+template <int MAXC>
 __device__ __forceinline__ void obj_sample(const float* plane, int w, int h, int c, double u, double v, double* out)
 {
     const double x = u * (double)w - 0.5, y = v * (double)h - 0.5;
@@ -40,9 +43,11 @@ __device__ __forceinline__ void obj_sample(const float* plane, int w, int h, int
     const float* e = plane + ((size_t)y1 * w + x0) * c;
     const float* f = plane + ((size_t)y1 * w + x1) * c;
     const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy), w01 = (1.0 - fx) * fy, w11 = fx * fy;
-    for (int k = 0; k < c; k++)
-        out[k] = w00 * (double)__ldg(a + k) + w10 * (double)__ldg(b + k) + w01 * (double)__ldg(e + k) +
-                 w11 * (double)__ldg(f + k);
+#pragma unroll
+    for (int k = 0; k < MAXC; k++)
+        if (k < c)
+            out[k] = w00 * (double)__ldg(a + k) + w10 * (double)__ldg(b + k) + w01 * (double)__ldg(e + k) +
+                     w11 * (double)__ldg(f + k);
 }
 
 __device__ __forceinline__ double block_sum(double v, double* sh)
@@ -61,15 +66,33 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
     return s;   // valid on thread 0
 }
 
+// One thread per pixel, its 1 + K sites in turn; each output row r formed in phi's order, b + sum of W[r][.] phi,
+// with phi = [c_q][s_i][s_i c_q] never stored: the row walks the three groups itself.
 __global__ void __launch_bounds__(OBJ_THREADS) k_objective(Planes P, ObjArgs A)
 {
-    __shared__ double sw[MAX_NOUT * MAX_NIN];
+    // The decoder at a fixed row stride of 24 feature slots, [c_q (4)][s_i (4)][s_i c_q (4 x 4)], whatever C0 and C1
+    // are: a channel the layout does not use has weight zero, whose product adds an exact zero to the row, so each row
+    // is the reference's sum over phi in phi's order and loads as twelve 16-byte pairs.
+    __shared__ __align__(16) double sw[MAX_NOUT * 24];
     __shared__ double sb[MAX_NOUT];
     __shared__ double scw[MAX_NOUT];
     __shared__ double red[32];
     const int nin = P.nin, nout = P.nout, c0 = P.c0, c1 = P.c1, kc = P.kc;
-    for (int i = threadIdx.x; i < nout * nin; i += blockDim.x)
-        sw[i] = (double)A.weights[i];
+    for (int i = threadIdx.x; i < nout * 24; i += blockDim.x)
+    {
+        const int r = i / 24, slot = i % 24;
+        int col = -1;
+        if (slot < 4)
+            col = slot < c1 ? slot : -1;
+        else if (slot < 8)
+            col = slot - 4 < c0 ? c1 + slot - 4 : -1;
+        else
+        {
+            const int ii = (slot - 8) / 4, q = (slot - 8) % 4;
+            col = ii < c0 && q < c1 ? c1 + c0 + ii * c1 + q : -1;
+        }
+        sw[i] = col >= 0 ? (double)A.weights[(size_t)r * nin + col] : 0.0;
+    }
     for (int i = threadIdx.x; i < nout; i += blockDim.x)
     {
         sb[i] = (double)A.bias[i];
@@ -92,29 +115,76 @@ __global__ void __launch_bounds__(OBJ_THREADS) k_objective(Planes P, ObjArgs A)
                 subtexel(kc, j - 1, px, py, dx, dy);
             const double u = ((double)px + 0.5 + (double)dx) / (double)V.w0;
             const double v = ((double)py + 0.5 + (double)dy) / (double)V.h0;
-            double s[MAX_CH], c[MAX_CH], t[MAX_NOUT];
-            obj_sample(V.v1, V.w1, V.h1, c1, u, v, c);
+            double s[MAX_CH], c[MAX_CH];
+#pragma unroll
+            for (int q = 0; q < MAX_CH; q++)
+            {
+                s[q] = 0.0;
+                c[q] = 0.0;
+            }
+            obj_sample<MAX_CH>(V.v1, V.w1, V.h1, c1, u, v, c);
+            // the source's taps at this site (the centre site reads the pixel itself)
+            size_t ta = (size_t)local * nout, tb = ta, te = ta, tf = ta;
+            double w00 = 1.0, w10 = 0.0, w01 = 0.0, w11 = 0.0;
             if (j == 0)
             {
-                for (int i = 0; i < c0; i++)
-                    s[i] = (double)V.v0[local * c0 + i];
-                for (int i = 0; i < nout; i++)
-                    t[i] = (double)__ldg(V.src + local * nout + i);
+#pragma unroll
+                for (int i = 0; i < MAX_CH; i++)
+                    if (i < c0)
+                        s[i] = (double)V.v0[local * c0 + i];
             }
             else
             {
-                obj_sample(V.v0, V.w0, V.h0, c0, u, v, s);
-                obj_sample(V.src, V.w0, V.h0, nout, u, v, t);
+                obj_sample<MAX_CH>(V.v0, V.w0, V.h0, c0, u, v, s);
+                const double x = u * (double)V.w0 - 0.5, y = v * (double)V.h0 - 0.5;
+                const double xf = floor(x), yf = floor(y);
+                const double fx = x - xf, fy = y - yf;
+                const int x0 = clampi((int)xf, V.w0), x1 = clampi((int)xf + 1, V.w0);
+                const int y0 = clampi((int)yf, V.h0), y1 = clampi((int)yf + 1, V.h0);
+                ta = ((size_t)y0 * V.w0 + x0) * nout;
+                tb = ((size_t)y0 * V.w0 + x1) * nout;
+                te = ((size_t)y1 * V.w0 + x0) * nout;
+                tf = ((size_t)y1 * V.w0 + x1) * nout;
+                w00 = (1.0 - fx) * (1.0 - fy);
+                w10 = fx * (1.0 - fy);
+                w01 = (1.0 - fx) * fy;
+                w11 = fx * fy;
             }
-            double phi[MAX_NIN];
-            features(s, c0, c, c1, phi);
+            double sc[16];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    sc[i * 4 + q] = s[i] * c[q];
             for (int r = 0; r < nout; r++)
             {
+                const double t = j == 0 ? (double)__ldg(V.src + ta + r)
+                                        : w00 * (double)__ldg(V.src + ta + r) + w10 * (double)__ldg(V.src + tb + r) +
+                                              w01 * (double)__ldg(V.src + te + r) + w11 * (double)__ldg(V.src + tf + r);
+                const double2* row = (const double2*)(sw + r * 24);
                 double acc = sb[r];
-                const double* row = sw + r * nin;
-                for (int i = 0; i < nin; i++)
-                    acc = fma(row[i], phi[i], acc);
-                const double e = acc - t[r];
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const double2 wv = row[h];
+                    acc = fma(wv.x, c[2 * h], acc);
+                    acc = fma(wv.y, c[2 * h + 1], acc);
+                }
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const double2 wv = row[2 + h];
+                    acc = fma(wv.x, s[2 * h], acc);
+                    acc = fma(wv.y, s[2 * h + 1], acc);
+                }
+#pragma unroll
+                for (int h = 0; h < 8; h++)
+                {
+                    const double2 wv = row[4 + h];
+                    acc = fma(wv.x, sc[2 * h], acc);
+                    acc = fma(wv.y, sc[2 * h + 1], acc);
+                }
+                const double e = acc - t;
                 weighted = fma(scw[r] * e, e, weighted);
                 if (j == 0)
                     centre = fma(e, e, centre);
