@@ -260,9 +260,12 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
     extern __shared__ double smem[];
     const int c0 = P.c0, n = 16 * c0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t per_warp = (size_t)n * n + 3 * (size_t)n + 16 + 16;
+    // A2's rows are padded to n + 1 doubles: a warp reading one COLUMN (a row per lane) then touches 32 different
+    // banks, where a stride of n doubles (a multiple of 32 words) would put all 32 lanes on one bank.
+    const int lda = n + 1;
+    const size_t per_warp = (size_t)n * lda + 3 * (size_t)n + 16 + 16;
     double* a2 = smem + warp * per_warp;
-    double* a1 = a2 + n * n;
+    double* a1 = a2 + n * lda;
     double* dv = a1 + n;
     double* uv = dv + n;
     double* dlt = uv + n;
@@ -285,7 +288,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
     const size_t T = (size_t)w0 * h0;
     const int cc = c0 * c0;
 
-    for (int i = lane; i < n * n; i += 32)
+    for (int i = lane; i < n * lda; i += 32)
         a2[i] = 0.0;
     for (int i = lane; i < n; i += 32)
     {
@@ -322,9 +325,9 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
                             for (int j = 0; j < c0; j++)
                             {
                                 const double e = B.stencil[(size_t)(slot * cc + i * c0 + j) * T + ti];
-                                a2[(size_t)(tid * c0 + i) * n + (ft * c0 + j)] += e;
+                                a2[(size_t)(tid * c0 + i) * lda + (ft * c0 + j)] += e;
                                 if (slot != 0)
-                                    a2[(size_t)(ft * c0 + j) * n + (tid * c0 + i)] += e;
+                                    a2[(size_t)(ft * c0 + j) * lda + (tid * c0 + i)] += e;
                             }
                     }
                     else
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
     {
         double s = 0.0;
         for (int j = 0; j < n; j++)
-            s += a2[(size_t)r * n + j] * dv[j];
+            s += a2[(size_t)r * lda + j] * dv[j];
         uv[r] = s;
     }
     const size_t gi = (size_t)gy * B.bx + gx;
@@ -388,7 +391,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
             double ap = 0.0, aq = 0.0;
             for (int j = 0; j < 16; j++)
             {
-                const double e = a2[(size_t)idx * n + (j * c0 + c)];
+                const double e = a2[(size_t)idx * lda + (j * c0 + c)];
                 const double aj = bc4_weight8(s_sel[c * 16 + j]);
                 ap += e * step * aj;
                 aq += e * step * (1.0 - aj);
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
             const int idx = lane * c0 + c;
             double quad = 0.0;
             for (int j = 0; j < 16; j++)
-                quad += a2[(size_t)idx * n + (j * c0 + c)] * dlt[j];
+                quad += a2[(size_t)idx * lda + (j * c0 + c)] * dlt[j];
             term = dlt[lane] * (2.0 * (a1[idx] + uv[idx]) + quad);
         }
         const double exact = fold16(term);
@@ -454,7 +457,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
             {
                 double add = 0.0;
                 for (int j = 0; j < 16; j++)
-                    add += a2[(size_t)r * n + (j * c0 + c)] * dlt[j];
+                    add += a2[(size_t)r * lda + (j * c0 + c)] * dlt[j];
                 uv[r] += add;
             }
             if (lane < 16)
@@ -480,7 +483,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
             for (int t = 0; t < 16; t++)
             {
                 const int i = t * c0 + c;
-                const double b = a1[i] + uv[i], a = a2[(size_t)i * n + i];
+                const double b = a1[i] + uv[i], a = a2[(size_t)i * lda + i];
                 const int cur = s_sel[c * 16 + t];
                 const double now = __shfl_sync(0xffffffffu, cand, cur);
                 const double d = cand - now;
@@ -501,7 +504,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
                 if (best < 0.0)
                 {
                     for (int r = lane; r < n; r += 32)
-                        uv[r] += a2[(size_t)r * n + i] * move;
+                        uv[r] += a2[(size_t)r * lda + i] * move;
                     if (lane == 0)
                     {
                         s_sel[c * 16 + t] = (unsigned char)which;
@@ -626,7 +629,7 @@ int bc_refine_passes(nntc_b200_device* d, const nntc_b200_model* m, int passes, 
     (void)m;
     double total = 0.0;
     const int n = 16 * d->c0;
-    const size_t per_warp = (size_t)n * n + 3 * (size_t)n + 32;
+    const size_t per_warp = (size_t)n * (n + 1) + 3 * (size_t)n + 32;
     const size_t shared = per_warp * REFINE_WARPS * sizeof(double);
     NB_CUDA(cudaFuncSetAttribute(k_bc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
     for (int pass = 0; pass < passes; pass++)
