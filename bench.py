@@ -149,6 +149,23 @@ def run_reference(args, rank, world):
     return 0
 
 
+def slowest(world, times_ms, device):
+    """Every rank's times, the max over ranks of each (the replicas' whole-job time is the slowest rank's)."""
+    import torch
+
+    t = torch.tensor(times_ms, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_value(world, mpix, steps, ms):
+    """Whole-job Mpix/s: every replica encodes `mpix` of base `steps` times within the slowest rank's `ms`."""
+    return world * mpix * steps / (ms / 1000.0)
+
+
 def big_material(seed):
     return materials.config(4, seed=seed)
 
@@ -255,13 +272,10 @@ def main():
         e2e_ms.append(ev0.elapsed_time(ev1))
     L.nntc_b200_device_destroy(handle)
 
-    mine = torch.tensor([device_ms, sum(e2e_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(mine, op=dist.ReduceOp.MAX)
-    device_ms, e2e_total = mine.tolist()
+    device_ms, e2e_total = slowest(world, [device_ms, sum(e2e_ms)], "cuda")
     mpix = mat.width * mat.height / 1e6
-    value = world * mpix * args.steps / (device_ms / 1000.0)
-    e2e_value = world * mpix * args.steps / (e2e_total / 1000.0)
+    value = job_value(world, mpix, args.steps, device_ms)
+    e2e_value = job_value(world, mpix, args.steps, e2e_total)
 
     if rank == 0:
         hbm, tf, src = peaks()
