@@ -213,6 +213,25 @@ long long nntc_b200_objective_passes(void);
 int nntc_b200_objective_check_host(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
                                    nntc_b200_objective* r);
 
+/* The objective of ONE plane held in the caller's own device memory, with no device allocation. This entry point has
+ * no counterpart in the reference: it serves a host that manages its plane buffers itself (a device model of its own,
+ * or memory committed to its own arena) and cannot afford nntc_b200_device_create's encode workspace or a cudaMalloc.
+ * Every pointer is device memory of the current device (or managed memory): v0 (w0 h0 c0), v1 (w1 h1 c1), src
+ * (w0 h0 nout), weights (nout x nin, row-major), bias (nout), cw (nout), and sums (3 doubles, written, need not start
+ * at zero): the cw-weighted sum over the 1 + k sites of every pixel, the unweighted centre-site sum and the unweighted
+ * sum over the k fractional sites - the three raw sums nntc_b200_objective_eval keeps per plane before it normalises
+ * them (e_plane = sums[0] / (sum cw (1 + k) w0 h0)). Both kernels are queued on `stream` (a cudaStream_t; 0 is the
+ * legacy default stream) and the call returns without waiting. The only scratch is a fixed static device array of
+ * 1.5 MiB, hence the limit of NNTC_B200_NOALLOC_MAX_PIXELS pixels per call; a larger plane is rejected with
+ * NNTC_B200_ERR_ARG and a message naming the limit. The first call on a device does its setup (it looks up the
+ * scratch's address, which loads the library's device code on that device) and should come before any stream capture.
+ * Calls in flight at the same time on one device (different streams, or host threads without ordering) share that
+ * scratch and race: order them, e.g. on one stream. */
+#define NNTC_B200_NOALLOC_MAX_PIXELS (4096LL * 4096LL)
+int nntc_b200_objective_plane_noalloc(const float* v0, int w0, int h0, int c0, const float* v1, int w1, int h1,
+                                      int c1, const float* src, int nout, const float* weights, const float* bias,
+                                      const float* cw, int nin, int k, double* sums, void* stream);
+
 /* ---- the BC refinement: src/refine_bc.cu:504-644. ep / sel are per-plane buffers of blocks*C0*2 and blocks*C0*16
  * bytes (block-major, then channel), exactly as the reference holds them. k0_host is the model's k0 mirror (what
  * the seed pack reads, src/export.cpp:294-328). ---- */

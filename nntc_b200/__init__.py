@@ -111,6 +111,7 @@ def check(status: int, what: str = "") -> None:
         raise NntcError(f"{what}: status {status}: {msg}")
 
 PROTOTYPES.update({
+    "nntc_b200_objective_plane_noalloc": (_I, [_P, _I, _I, _I, _P, _I, _I, _I, _P, _I, _P, _P, _P, _I, _I, _P, _P]),
     "nntc_b200_launch_count": (C.c_longlong, []),
     "nntc_b200_kernel_timing": (_I, [_P, _I]),
     "nntc_b200_kernel_stats": (_I, [_P, _I, C.POINTER(C.c_longlong), _PD, _I]),

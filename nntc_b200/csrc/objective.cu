@@ -11,6 +11,8 @@
 // in the last bits only, and E is a measurement held to 1e-9 relative of the host twin (src/objective.cu:317-380).
 
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "device.cuh"
@@ -411,3 +413,133 @@ int nntc_b200_objective_check_host(nntc_b200_device* d, const nntc_b200_model* m
 }
 
 }   // extern "C"
+
+// ---- the objective of one caller-owned plane, with no device allocation -------------------------------------------
+//
+// Who calls this: a host that keeps a plane in device memory it manages itself - the reference's own device model,
+// which owns every plane buffer of its chain, or a process whose device memory is already committed to its own arena
+// - and wants E of that plane without building a device model. nntc_b200_device_create allocates the whole encode
+// workspace of a chain (stencils, CG vectors, partials: tens of GB at 4096 x 4096), and cudaMalloc both blocks the
+// device and may simply fail under such a budget. Here the inputs and the three sums are the caller's memory; the only
+// scratch is the per-block partials of k_objective, held in a fixed static device array of NOALLOC_MAX_BLOCKS * 3
+// doubles (1.5 MiB), which bounds one call at NNTC_B200_NOALLOC_MAX_PIXELS pixels.
+
+namespace nb
+{
+
+constexpr long long NOALLOC_MAX_BLOCKS = NNTC_B200_NOALLOC_MAX_PIXELS / OBJ_THREADS;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+// Every word a call reads is written earlier in the same call (k_objective writes each block's three partials,
+// k_objective_reduce reads only those), so nothing here needs to start at zero.
+static __device__ __align__(256) double g_noalloc_partial[3 * NOALLOC_MAX_BLOCKS];
+
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+// The scratch's device address on the current device, looked up once per device with that device current.
+static int noalloc_scratch(double** out)
+{
+    int dev = -1;
+    NB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    {
+        set_error(NNTC_B200_ERR_ARG, "objective_plane_noalloc: device ordinal " + std::to_string(dev) +
+                                         " is beyond the " + std::to_string(NOALLOC_MAX_DEVICES) + " it keeps");
+        return NNTC_B200_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev])
+    {
+        void* p = nullptr;
+        NB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partial));
+        g_noalloc_addr[dev] = (double*)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return NNTC_B200_OK;
+}
+
+// A pointer the kernels may read or write on the current device: device memory of this device, or managed memory.
+static int noalloc_pointer(const void* p, const char* name)
+{
+    if (!p)
+    {
+        set_error(NNTC_B200_ERR_ARG, std::string("objective_plane_noalloc: ") + name + " is null");
+        return NNTC_B200_ERR_ARG;
+    }
+    cudaPointerAttributes a{};
+    NB_CUDA(cudaPointerGetAttributes(&a, p));
+    int dev = -1;
+    NB_CUDA(cudaGetDevice(&dev));
+    const bool ok = a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
+    if (!ok)
+    {
+        set_error(NNTC_B200_ERR_ARG,
+                  std::string("objective_plane_noalloc: ") + name + " is not device memory of the current device");
+        return NNTC_B200_ERR_ARG;
+    }
+    return NNTC_B200_OK;
+}
+
+}   // namespace nb
+
+extern "C" int nntc_b200_objective_plane_noalloc(const float* v0, int w0, int h0, int c0, const float* v1, int w1,
+                                                 int h1, int c1, const float* src, int nout, const float* weights,
+                                                 const float* bias, const float* cw, int nin, int k, double* sums,
+                                                 void* stream)
+{
+    auto bad = [](const std::string& what) {
+        set_error(NNTC_B200_ERR_ARG, "objective_plane_noalloc: " + what);
+        return (int)NNTC_B200_ERR_ARG;
+    };
+    if (w0 < 1 || h0 < 1 || w1 < 1 || h1 < 1)
+        return bad("plane sizes must be positive");
+    if ((long long)w0 * h0 > NNTC_B200_NOALLOC_MAX_PIXELS)
+        return bad(std::to_string((long long)w0 * h0) + " pixels is above the limit of " +
+                   std::to_string((long long)NNTC_B200_NOALLOC_MAX_PIXELS) + " (its static scratch holds " +
+                   std::to_string(NOALLOC_MAX_BLOCKS) + " blocks of " + std::to_string(OBJ_THREADS) + ")");
+    if (c0 < 1 || c0 > MAX_CH || c1 < 1 || c1 > MAX_CH)
+        return bad("channel counts must be 1.." + std::to_string(MAX_CH));
+    if (nout < 1 || nout > MAX_NOUT)
+        return bad("nout must be 1.." + std::to_string(MAX_NOUT));
+    if (nin != c1 + c0 + c0 * c1)
+        return bad("nin must be c1 + c0 + c0 c1");
+    if (k != 0 && k != 1 && k != 2 && k != 4)
+        return bad("k must be 0, 1, 2 or 4");
+    NB_TRY(noalloc_pointer(v0, "v0"));
+    NB_TRY(noalloc_pointer(v1, "v1"));
+    NB_TRY(noalloc_pointer(src, "src"));
+    NB_TRY(noalloc_pointer(weights, "weights"));
+    NB_TRY(noalloc_pointer(bias, "bias"));
+    NB_TRY(noalloc_pointer(cw, "cw"));
+    NB_TRY(noalloc_pointer(sums, "sums"));
+    double* partial = nullptr;
+    NB_TRY(noalloc_scratch(&partial));
+
+    Planes P{};
+    P.n = 1;
+    P.c0 = c0;
+    P.c1 = c1;
+    P.nin = nin;
+    P.nout = nout;
+    P.kc = k;
+    P.c = c0;
+    PlaneView& v = P.p[0];
+    v.w0 = w0;
+    v.h0 = h0;
+    v.w1 = w1;
+    v.h1 = h1;
+    v.src = src;
+    v.v0 = const_cast<float*>(v0);   // read only: k_objective writes nothing but its partials
+    v.v1 = const_cast<float*>(v1);
+    const long long pixels = (long long)w0 * h0;
+    P.start[0] = 0;
+    P.start[1] = (pixels + OBJ_THREADS - 1) / OBJ_THREADS * OBJ_THREADS;
+    const int nblocks = (int)(P.start[1] / OBJ_THREADS);
+    const cudaStream_t s = (cudaStream_t)stream;
+    k_objective<<<nblocks, OBJ_THREADS, 0, s>>>(P, ObjArgs{ weights, bias, cw, partial });
+    NB_LAUNCHED();
+    k_objective_reduce<<<1, 256, 0, s>>>(P, partial, nblocks, sums);
+    NB_LAUNCHED();
+    return NNTC_B200_OK;
+}
