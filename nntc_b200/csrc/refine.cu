@@ -236,6 +236,62 @@ __global__ void k_bc_decode(BcPlanes P, const float* lo0, const float* hi0)
     }
 }
 
+// The layout of one warp's block in shared memory, per level-0 channel count.
+//
+// A2 couples a texel only with itself and its eight neighbours (the 9-point stencil), so it is held as the sixteen
+// texels' five OWNED stencil blocks, S[texel][slot][i][j] (the texel stride padded to an odd number of doubles), and
+// an entry A2[(t, i)][(u, j)] is read from t's block when u sits at one of t's owned offsets, else from u's block,
+// transposed. Every sum over a row of A2 visits only the entries that can be nonzero, in column order: such a sum
+// starts at +0.0 and so never holds -0.0, and adding the product of a structural zero would leave it bit-for-bit
+// unchanged. The vector u = A2 d lives in registers, R rows per lane.
+template <int C0>
+struct RefineShape
+{
+    static constexpr int N = 16 * C0;              // unknowns of the block: (texel, channel), texel-major
+    static constexpr int R = (N + 31) / 32;        // rows of u per lane: row r = lane + 32 q
+    static constexpr int CC = C0 * C0;
+    static constexpr int TS = (5 * CC) | 1;        // doubles per texel of S
+    static constexpr int PER_WARP = 16 * TS + 2 * N + 16 + 8 + 16;   // S, a1, d, dlt, the weights, ep and sel
+};
+
+// The entry of A2 at row (t, i), column (u, j), where u is t's neighbour number k (k = (dy + 1) 3 + (dx + 1), the
+// neighbours' order by texel index).
+template <int C0>
+__device__ __forceinline__ double a2_entry(const double* S, int t, int i, int u, int j, int k)
+{
+    using Sh = RefineShape<C0>;
+    return k >= 4 ? S[t * Sh::TS + (k - 4) * Sh::CC + i * C0 + j] : S[u * Sh::TS + (4 - k) * Sh::CC + j * C0 + i];
+}
+
+// Neighbour k of in-block texel t, or -1 outside the block.
+__device__ __forceinline__ int block_neighbour(int t, int k)
+{
+    const int x = (t & 3) + k % 3 - 1, y = (t >> 2) + k / 3 - 1;
+    return x >= 0 && x < 4 && y >= 0 && y < 4 ? y * 4 + x : -1;
+}
+
+// Which neighbour of texel t texel u is, or -1.
+__device__ __forceinline__ int neighbour_index(int t, int u)
+{
+    const int dx = (u & 3) - (t & 3), dy = (u >> 2) - (t >> 2);
+    return dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 ? (dy + 1) * 3 + (dx + 1) : -1;
+}
+
+// Row idx of u, from the lane that holds it (every lane takes part; the value is meaningful on every lane).
+template <int R>
+__device__ __forceinline__ double row_of(const double (&uv)[R], int idx)
+{
+    double v = 0.0;
+#pragma unroll
+    for (int q = 0; q < R; q++)
+    {
+        const double x = __shfl_sync(0xffffffffu, uv[q], idx & 31);
+        if ((idx >> 5) == q)
+            v = x;
+    }
+    return v;
+}
+
 // The sixteen lanes' terms folded serially in texel order, the same on every lane.
 __device__ __forceinline__ double fold16(double v)
 {
@@ -253,24 +309,22 @@ struct RefineArgs
     double* stats;   // [plane][2]
 };
 
-// One warp per 4x4 block of the colour; the block of every plane of the chain in one launch (start[] counts blocks
+// One warp per 4x4 block of the colour; the blocks of every plane of the chain in one launch (start[] counts blocks
 // of the colour per plane).
-__global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, RefineArgs R)
+template <int C0>
+__global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, RefineArgs R)
 {
+    using Sh = RefineShape<C0>;
+    constexpr int N = Sh::N, RR = Sh::R, TS = Sh::TS, CC = Sh::CC;
     extern __shared__ double smem[];
-    const int c0 = P.c0, n = 16 * c0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // A2's rows are padded to n + 1 doubles: a warp reading one COLUMN (a row per lane) then touches 32 different
-    // banks, where a stride of n doubles (a multiple of 32 words) would put all 32 lanes on one bank.
-    const int lda = n + 1;
-    const size_t per_warp = (size_t)n * lda + 3 * (size_t)n + 16 + 16;
-    double* a2 = smem + warp * per_warp;
-    double* a1 = a2 + n * lda;
-    double* dv = a1 + n;
-    double* uv = dv + n;
-    double* dlt = uv + n;
-    int* s_ep = (int*)(dlt + 16);            // 8 ints
-    unsigned char* s_sel = (unsigned char*)(s_ep + 8);   // 64 bytes (fits in the last 16 doubles with s_ep)
+    double* S = smem + warp * Sh::PER_WARP;
+    double* a1 = S + 16 * TS;
+    double* dv = a1 + N;
+    double* dlt = dv + N;
+    double* w8 = dlt + 16;
+    int* s_ep = (int*)(w8 + 8);                          // 8 ints
+    unsigned char* s_sel = (unsigned char*)(s_ep + 8);   // 64 bytes
 
     const long long bi = (long long)blockIdx.x * REFINE_WARPS + warp;
     if (bi >= P.start[P.n])
@@ -286,113 +340,113 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
     const int gy = R.cy + 2 * (int)(local / cbx);
     const int w0 = B.w0, h0 = B.h0;
     const size_t T = (size_t)w0 * h0;
-    const int cc = c0 * c0;
 
-    for (int i = lane; i < n * lda; i += 32)
-        a2[i] = 0.0;
-    for (int i = lane; i < n; i += 32)
+    // The block's quadratic (src/cpu/cpu_refine_bc.cpp:152-205), one lane per row (texel, channel): the row's owned
+    // stencil blocks whose partner lies in the block go to S, the rest of the stencil meets the neighbours'
+    // corrections in the row's share of A1, summed in the reference's order (per slot: the owned block, then the
+    // neighbour's transposed one).
+#pragma unroll
+    for (int q = 0; q < RR; q++)
     {
-        a1[i] = 0.0;
-        dv[i] = 0.0;
-        uv[i] = 0.0;
-    }
-    __syncwarp();
-
-    // The block's quadratic, one lane per texel (src/cpu/cpu_refine_bc.cpp:152-205). Every A2 entry receives exactly
-    // one contribution, so the parallel writes need no order.
-    if (lane < 16)
-    {
-        const int tid = lane;
-        const int px = gx * 4 + (tid & 3), py = gy * 4 + (tid >> 2);
-        if (px < w0 && py < h0)
+        const int r = lane + 32 * q;
+        if (r >= N)
+            continue;
+        const int t = r / C0, i = r % C0;
+        const int px = gx * 4 + (t & 3), py = gy * 4 + (t >> 2);
+        const bool in = px < w0 && py < h0;
+        const size_t ti = in ? (size_t)py * w0 + px : 0;
+        double acc = in ? B.grad[ti * C0 + i] : 0.0;
+        for (int slot = 0; slot < SLOTS; slot++)
         {
-            const size_t ti = (size_t)py * w0 + px;
-            double acc[MAX_CH];
-            for (int i = 0; i < c0; i++)
-                acc[i] = B.grad[ti * c0 + i];
-            for (int slot = 0; slot < SLOTS; slot++)
+            int dx, dy;
+            slot_offset(slot, dx, dy);
+            const int fx = px + dx, fy = py + dy;
+            const bool f_img = in && fx >= 0 && fx < w0 && fy >= 0 && fy < h0;
+            const int lx = fx - gx * 4, ly = fy - gy * 4;
+            const bool f_blk = lx >= 0 && lx < 4 && ly >= 0 && ly < 4;
+            double* s_row = S + t * TS + slot * CC + i * C0;
+            for (int j = 0; j < C0; j++)
+                s_row[j] = f_img && f_blk ? B.stencil[(size_t)(slot * CC + i * C0 + j) * T + ti] : 0.0;
+            if (f_img && !f_blk)
             {
-                int dx, dy;
-                slot_offset(slot, dx, dy);
-                const int fx = px + dx, fy = py + dy;
-                if (fx >= 0 && fx < w0 && fy >= 0 && fy < h0)
-                {
-                    const int lx = fx - gx * 4, ly = fy - gy * 4;
-                    if (lx >= 0 && lx < 4 && ly >= 0 && ly < 4)
-                    {
-                        const int ft = ly * 4 + lx;
-                        for (int i = 0; i < c0; i++)
-                            for (int j = 0; j < c0; j++)
-                            {
-                                const double e = B.stencil[(size_t)(slot * cc + i * c0 + j) * T + ti];
-                                a2[(size_t)(tid * c0 + i) * lda + (ft * c0 + j)] += e;
-                                if (slot != 0)
-                                    a2[(size_t)(ft * c0 + j) * lda + (tid * c0 + i)] += e;
-                            }
-                    }
-                    else
-                    {
-                        const double* xn = B.delta + ((size_t)fy * w0 + fx) * c0;
-                        for (int i = 0; i < c0; i++)
-                            for (int j = 0; j < c0; j++)
-                                acc[i] += B.stencil[(size_t)(slot * cc + i * c0 + j) * T + ti] * xn[j];
-                    }
-                }
-                if (slot == 0)
-                    continue;
-                const int ax = px - dx, ay = py - dy;
-                const int lx = ax - gx * 4, ly = ay - gy * 4;
-                if (ax < 0 || ax >= w0 || ay < 0 || ay >= h0 || (lx >= 0 && lx < 4 && ly >= 0 && ly < 4))
-                    continue;
-                const size_t nt = (size_t)ay * w0 + ax;
-                const double* xn = B.delta + nt * c0;
-                for (int i = 0; i < c0; i++)
-                    for (int j = 0; j < c0; j++)
-                        acc[i] += B.stencil[(size_t)(slot * cc + j * c0 + i) * T + nt] * xn[j];
+                const double* xn = B.delta + ((size_t)fy * w0 + fx) * C0;
+                for (int j = 0; j < C0; j++)
+                    acc += B.stencil[(size_t)(slot * CC + i * C0 + j) * T + ti] * xn[j];
             }
-            for (int i = 0; i < c0; i++)
-            {
-                a1[tid * c0 + i] = acc[i];
-                dv[tid * c0 + i] = (double)B.v0[ti * c0 + i] - (double)B.prev[ti * c0 + i];
-            }
+            if (slot == 0 || !in)
+                continue;
+            const int ax = px - dx, ay = py - dy;
+            const int mx = ax - gx * 4, my = ay - gy * 4;
+            if (ax < 0 || ax >= w0 || ay < 0 || ay >= h0 || (mx >= 0 && mx < 4 && my >= 0 && my < 4))
+                continue;
+            const size_t nt = (size_t)ay * w0 + ax;
+            const double* xn = B.delta + nt * C0;
+            for (int j = 0; j < C0; j++)
+                acc += B.stencil[(size_t)(slot * CC + j * C0 + i) * T + nt] * xn[j];
         }
-    }
-    __syncwarp();
-    for (int r = lane; r < n; r += 32)
-    {
-        double s = 0.0;
-        for (int j = 0; j < n; j++)
-            s += a2[(size_t)r * lda + j] * dv[j];
-        uv[r] = s;
+        a1[r] = acc;
+        dv[r] = in ? (double)B.v0[ti * C0 + i] - (double)B.prev[ti * C0 + i] : 0.0;
     }
     const size_t gi = (size_t)gy * B.bx + gx;
-    if (lane < c0)
+    if (lane < C0)
     {
-        s_ep[2 * lane] = B.ep[(gi * c0 + lane) * 2];
-        s_ep[2 * lane + 1] = B.ep[(gi * c0 + lane) * 2 + 1];
+        s_ep[2 * lane] = B.ep[(gi * C0 + lane) * 2];
+        s_ep[2 * lane + 1] = B.ep[(gi * C0 + lane) * 2 + 1];
     }
-    for (int i = lane; i < n; i += 32)
-        s_sel[i] = B.sel[gi * c0 * 16 + i];
+    for (int i = lane; i < N; i += 32)
+        s_sel[i] = B.sel[gi * C0 * 16 + i];
+    if (lane < 8)
+        w8[lane] = bc4_weight8(lane);
     __syncwarp();
 
+    // u = A2 d, row by row in column order
+    double uv[RR];
+#pragma unroll
+    for (int q = 0; q < RR; q++)
+    {
+        uv[q] = 0.0;
+        const int r = lane + 32 * q;
+        if (r >= N)
+            continue;
+        const int t = r / C0, i = r % C0;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; k++)
+        {
+            const int u = block_neighbour(t, k);
+            if (u < 0)
+                continue;
+#pragma unroll
+            for (int j = 0; j < C0; j++)
+                s += a2_entry<C0>(S, t, i, u, j, k) * dv[u * C0 + j];
+        }
+        uv[q] = s;
+    }
+
     double taken = 0.0;
+    const int t16 = lane & 15;
     // ---- (i) the endpoints of each channel (src/cpu/cpu_refine_bc.cpp:222-312)
-    for (int c = 0; c < c0; c++)
+    for (int c = 0; c < C0; c++)
     {
         const double step = ((double)R.hi0[c] - (double)R.lo0[c]) / 255.0;
+        const int idx = t16 * C0 + c;
+        const double u_idx = row_of(uv, idx);
         double tbp = 0.0, tbq = 0.0, tpap = 0.0, tpaq = 0.0, tqaq = 0.0;
         if (lane < 16)
         {
-            const int idx = lane * c0 + c;
-            const double a = bc4_weight8(s_sel[c * 16 + lane]);
+            const double a = w8[s_sel[c * 16 + lane]];
             const double p = step * a;
             const double q = step * (1.0 - a);
-            const double b = a1[idx] + uv[idx];
+            const double b = a1[idx] + u_idx;
             double ap = 0.0, aq = 0.0;
-            for (int j = 0; j < 16; j++)
+#pragma unroll
+            for (int k = 0; k < 9; k++)
             {
-                const double e = a2[(size_t)idx * lda + (j * c0 + c)];
-                const double aj = bc4_weight8(s_sel[c * 16 + j]);
+                const int u = block_neighbour(lane, k);
+                if (u < 0)
+                    continue;
+                const double e = a2_entry<C0>(S, lane, c, u, c, k);
+                const double aj = w8[s_sel[c * 16 + u]];
                 ap += e * step * aj;
                 aq += e * step * (1.0 - aj);
             }
@@ -444,24 +498,36 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
         double term = 0.0;
         if (lane < 16)
         {
-            const int idx = lane * c0 + c;
             double quad = 0.0;
-            for (int j = 0; j < 16; j++)
-                quad += a2[(size_t)idx * lda + (j * c0 + c)] * dlt[j];
-            term = dlt[lane] * (2.0 * (a1[idx] + uv[idx]) + quad);
+#pragma unroll
+            for (int k = 0; k < 9; k++)
+            {
+                const int u = block_neighbour(lane, k);
+                if (u >= 0)
+                    quad += a2_entry<C0>(S, lane, c, u, c, k) * dlt[u];
+            }
+            term = dlt[lane] * (2.0 * (a1[idx] + u_idx) + quad);
         }
         const double exact = fold16(term);
         if (exact < 0.0)
         {
-            for (int r = lane; r < n; r += 32)
+#pragma unroll
+            for (int q = 0; q < RR; q++)
             {
+                const int r = lane + 32 * q;
+                if (r >= N)
+                    continue;
+                const int t = r / C0, i = r % C0;
                 double add = 0.0;
-                for (int j = 0; j < 16; j++)
-                    add += a2[(size_t)r * lda + (j * c0 + c)] * dlt[j];
-                uv[r] += add;
+#pragma unroll
+                for (int k = 0; k < 9; k++)
+                {
+                    const int u = block_neighbour(t, k);
+                    if (u >= 0)
+                        add += a2_entry<C0>(S, t, i, u, c, k) * dlt[u];
+                }
+                uv[q] += add;
             }
-            if (lane < 16)
-                dv[lane * c0 + c] += dlt[lane];
             if (lane == 0)
             {
                 s_ep[2 * c] = best0;
@@ -472,69 +538,81 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_bc_refine(BcPlanes P, Ref
         __syncwarp();
     }
 
-    // ---- (ii) the selectors: two Gauss-Seidel passes of exact 8-way argmins (src/cpu/cpu_refine_bc.cpp:314-345)
+    // ---- (ii) the selectors: two Gauss-Seidel passes of exact 8-way argmins (src/cpu/cpu_refine_bc.cpp:314-345).
+    // Every group of eight lanes evaluates the eight candidates, one per lane, and takes the lowest change in three
+    // butterfly rounds, ties to the lower candidate: the candidate the reference's in-order scan with a strict `<`
+    // keeps, and no candidate when none lowers E.
+    const int k8 = lane & 7;
     for (int pass = 0; pass < 2; pass++)
-        for (int c = 0; c < c0; c++)
+        for (int c = 0; c < C0; c++)
         {
             const int r0 = s_ep[2 * c], r1 = s_ep[2 * c + 1];
-            const float lo = R.lo0[c], hi = R.hi0[c];
-            // the eight decoded values of this channel's palette, one per lane 0..7
-            const double cand = lane < 8 ? (double)bc0_value(lo, hi, bc4_entry(r0, r1, lane)) : 0.0;
+            const double cand = (double)bc0_value(R.lo0[c], R.hi0[c], bc4_entry(r0, r1, k8));
             for (int t = 0; t < 16; t++)
             {
-                const int i = t * c0 + c;
-                const double b = a1[i] + uv[i], a = a2[(size_t)i * lda + i];
+                const int i = t * C0 + c;
+                const double b = a1[i] + row_of(uv, i);
+                const double a = S[t * TS + c * C0 + c];
                 const int cur = s_sel[c * 16 + t];
                 const double now = __shfl_sync(0xffffffffu, cand, cur);
                 const double d = cand - now;
                 const double de = 2.0 * b * d + a * d * d;
-                double best = 0.0, move = 0.0;
-                int which = cur;
-                for (int kk = 0; kk < 8; kk++)
+                double v = de < 0.0 ? de : 0.0, mv = d;
+                int id = de < 0.0 ? k8 : 8;
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1)
                 {
-                    const double dk = __shfl_sync(0xffffffffu, de, kk);
-                    if (dk < best)
+                    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                    const double om = __shfl_xor_sync(0xffffffffu, mv, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, id, o);
+                    if (ov < v || (ov == v && oi < id))
                     {
-                        best = dk;
-                        move = __shfl_sync(0xffffffffu, d, kk);
-                        which = kk;
+                        v = ov;
+                        mv = om;
+                        id = oi;
                     }
                 }
-                // move and which are uniform: every lane ran the same scan over the same shuffled values
-                if (best < 0.0)
+                // v, mv and id are the same on every lane
+                if (v < 0.0)
                 {
-                    for (int r = lane; r < n; r += 32)
-                        uv[r] += a2[(size_t)r * lda + i] * move;
-                    if (lane == 0)
+#pragma unroll
+                    for (int q = 0; q < RR; q++)
                     {
-                        s_sel[c * 16 + t] = (unsigned char)which;
-                        dv[i] += move;
+                        const int r = lane + 32 * q;
+                        if (r >= N)
+                            continue;
+                        const int rt = r / C0, ri = r % C0;
+                        const int k = neighbour_index(rt, t);
+                        if (k >= 0)
+                            uv[q] += a2_entry<C0>(S, rt, ri, t, c, k) * mv;
                     }
-                    taken += best;
+                    if (lane == 0)
+                        s_sel[c * 16 + t] = (unsigned char)id;
+                    taken += v;
                 }
                 __syncwarp();
             }
         }
 
     // ---- what the block leaves behind
-    if (lane < c0)
+    if (lane < C0)
     {
-        B.ep[(gi * c0 + lane) * 2] = (uint8_t)s_ep[2 * lane];
-        B.ep[(gi * c0 + lane) * 2 + 1] = (uint8_t)s_ep[2 * lane + 1];
+        B.ep[(gi * C0 + lane) * 2] = (uint8_t)s_ep[2 * lane];
+        B.ep[(gi * C0 + lane) * 2 + 1] = (uint8_t)s_ep[2 * lane + 1];
     }
-    for (int i = lane; i < n; i += 32)
-        B.sel[gi * c0 * 16 + i] = s_sel[i];
+    for (int i = lane; i < N; i += 32)
+        B.sel[gi * C0 * 16 + i] = s_sel[i];
     if (lane < 16)
     {
         const int px = gx * 4 + (lane & 3), py = gy * 4 + (lane >> 2);
         if (px < w0 && py < h0)
         {
             const size_t ti = (size_t)py * w0 + px;
-            for (int c = 0; c < c0; c++)
+            for (int c = 0; c < C0; c++)
             {
                 const float byte = bc4_entry(s_ep[2 * c], s_ep[2 * c + 1], s_sel[c * 16 + lane]);
                 const float value = bc0_value(R.lo0[c], R.hi0[c], byte);
-                const size_t idx = ti * c0 + c;
+                const size_t idx = ti * C0 + c;
                 B.v0[idx] = value;
                 B.k0[idx] = bc0_index(byte);
                 B.delta[idx] = (double)value - (double)B.prev[idx];
@@ -628,10 +706,19 @@ int bc_refine_passes(nntc_b200_device* d, const nntc_b200_model* m, int passes, 
 {
     (void)m;
     double total = 0.0;
-    const int n = 16 * d->c0;
-    const size_t per_warp = (size_t)n * (n + 1) + 3 * (size_t)n + 32;
-    const size_t shared = per_warp * REFINE_WARPS * sizeof(double);
-    NB_CUDA(cudaFuncSetAttribute(k_bc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
+    const int c0 = d->c0;
+    if (c0 < 1 || c0 > MAX_CH)
+    {
+        set_error(NNTC_B200_ERR_STATE, "the BC refinement needs 1..4 level-0 channels");
+        return NNTC_B200_ERR_STATE;
+    }
+    const int per_warp = c0 == 1 ? RefineShape<1>::PER_WARP
+                                 : (c0 == 2 ? RefineShape<2>::PER_WARP
+                                            : (c0 == 3 ? RefineShape<3>::PER_WARP : RefineShape<4>::PER_WARP));
+    const size_t shared = (size_t)per_warp * REFINE_WARPS * sizeof(double);
+    void (*kernel)(BcPlanes, RefineArgs) =
+        c0 == 1 ? k_bc_refine<1> : (c0 == 2 ? k_bc_refine<2> : (c0 == 3 ? k_bc_refine<3> : k_bc_refine<4>));
+    NB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
     for (int pass = 0; pass < passes; pass++)
     {
         NB_CUDA(cudaMemsetAsync(d->bc_stats, 0, (size_t)MAX_PLANES * 2 * sizeof(double), d->stream));
@@ -649,7 +736,7 @@ int bc_refine_passes(nntc_b200_device* d, const nntc_b200_model* m, int passes, 
             RefineArgs R{ d->lo0, d->hi0, cx, cy, d->bc_stats };
             const int grid = grid_for((size_t)P.start[P.n], REFINE_WARPS);
             NB_TRY(ktimer_begin(d, NNTC_B200_K_REFINE));
-            k_bc_refine<<<grid, 32 * REFINE_WARPS, shared, d->stream>>>(P, R);
+            kernel<<<grid, 32 * REFINE_WARPS, shared, d->stream>>>(P, R);
             NB_TRY(ktimer_end(d));
             NB_LAUNCHED();
         }

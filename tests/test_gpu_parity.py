@@ -191,7 +191,7 @@ def test_assembly_and_objective_vs_oracle(textures, c0, c1, w, h):
                 assert np.array_equal(ws["stencil"], sten) and np.array_equal(ws["grad"], grad), (level0, i)
 
 
-@pytest.mark.parametrize("textures,c0,c1,w,h", SIZES[:2])
+@pytest.mark.parametrize("textures,c0,c1,w,h", SIZES + [(1, 3, 2, 45, 29)])
 def test_bc_refine_vs_oracle(textures, c0, c1, w, h):
     from nntc_b200 import lib, check
     mat = materials.small(31 + w, w, h, textures=textures, c0=c0, c1=c1)
