@@ -43,17 +43,25 @@ __host__ __device__ constexpr int pair_k(int p)
 
 struct SiteArgs
 {
-    const float* weights;
-    const float* bias;
-    const float* cw;
     double* terms;                      // [site][c] over every plane
+    float4* y;                          // [site]: the site's sample of the other latent
     long long site0[MAX_PLANES + 1];    // the first site of each plane in `terms`
 };
 
 // One thread per site: t_s[a] = sum_r cw_r G[r][a] res_r (level 1, block b) or sum_r cw_r Q[r][a] res_r (level 0,
 // block c'), in the reference's order of operations (src/solve_level1.cu:335-361, 518-544).
-template <bool LEVEL0>
-__global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs A)
+// The decoder as a launch parameter, each row at a fixed stride of 24 slots, [c_q (4)][s_i (4)][s_i c_q (4 x 4)]: with
+// the row loop unrolled every weight is a constant-bank operand. Slots of channels the layout does not use are never
+// read (the channel loops are guarded), so the arithmetic is the reference's operation for operation.
+struct SiteDecoder
+{
+    float w[MAX_NOUT * 24];
+    float b[MAX_NOUT];
+    float cw[MAX_NOUT];
+};
+
+template <bool LEVEL0, int NOUT>
+__global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs A, SiteDecoder W)
 {
     const long long base = (long long)blockIdx.x * blockDim.x;
     const int pl = plane_of(P, base);
@@ -62,7 +70,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
     const int kc = P.kc, per = 1 + kc;
     if (si >= (long long)V.w0 * V.h0 * per)
         return;
-    const int c0 = P.c0, c1 = P.c1, nin = P.nin, nout = P.nout;
+    const int c0 = P.c0, c1 = P.c1;
     const long long pixel = si / per;
     const int j = (int)(si % per);
     const int px = (int)(pixel % V.w0), py = (int)(pixel / V.w0);
@@ -90,29 +98,30 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
 #pragma unroll
     for (int a = 0; a < MAX_CH; a++)
         acc[a] = 0.0;
-    for (int r = 0; r < nout; r++)
+#pragma unroll
+    for (int r = 0; r < NOUT; r++)
     {
         // the target of this output, sampled as blend() samples it
         float target;
         if (j == 0)
-            target = __ldg(V.src + pixel * nout + r);
+            target = __ldg(V.src + pixel * NOUT + r);
         else
         {
             const float* s = V.src + r;
-            target = w0[0] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x0) * nout) +
-                     w0[1] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x1) * nout) +
-                     w0[2] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x0) * nout) +
-                     w0[3] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x1) * nout);
+            target = w0[0] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x0) * NOUT) +
+                     w0[1] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x1) * NOUT) +
+                     w0[2] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x0) * NOUT) +
+                     w0[3] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x1) * NOUT);
         }
-        const float* row = A.weights + (size_t)r * nin;
-        float out = A.bias[r];
+        const float* row = W.w + r * 24;   // [c_q][s_i][s_i c_q]
+        float out = W.b[r];
         float col[MAX_CH];
         if (!LEVEL0)
         {
 #pragma unroll
             for (int i = 0; i < MAX_CH; i++)
                 if (i < c0)
-                    out += row[c1 + i] * sbar[i];
+                    out += row[4 + i] * sbar[i];
 #pragma unroll
             for (int q = 0; q < MAX_CH; q++)
                 if (q < c1)
@@ -121,7 +130,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
 #pragma unroll
                     for (int i = 0; i < MAX_CH; i++)
                         if (i < c0)
-                            gg += sbar[i] * row[c1 + c0 + i * c1 + q];
+                            gg += sbar[i] * row[8 + i * 4 + q];
                     col[q] = gg;
                     out += gg * cbar[q];
                 }
@@ -136,11 +145,11 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
             for (int i = 0; i < MAX_CH; i++)
                 if (i < c0)
                 {
-                    float qq = row[c1 + i];
+                    float qq = row[4 + i];
 #pragma unroll
                     for (int q = 0; q < MAX_CH; q++)
                         if (q < c1)
-                            qq += cbar[q] * row[c1 + c0 + i * c1 + q];
+                            qq += cbar[q] * row[8 + i * 4 + q];
                     col[i] = qq;
                     out += qq * sbar[i];
                 }
@@ -150,7 +159,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
 #pragma unroll
         for (int a = 0; a < MAX_CH; a++)
             if (a < c)
-                acc[a] += (double)A.cw[r] * (double)col[a] * (double)res;
+                acc[a] += (double)W.cw[r] * (double)col[a] * (double)res;
     }
     const int c = LEVEL0 ? c0 : c1;
     double* out_t = A.terms + (size_t)(A.site0[pl] + si) * c;
@@ -158,6 +167,13 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
     for (int a = 0; a < MAX_CH; a++)
         if (a < c)
             out_t[a] = acc[a];
+    // the other latent's sample, which every (texel, slot) of the gather that meets this site needs again
+    float y[MAX_CH];
+    const int ny = LEVEL0 ? c1 : c0;
+#pragma unroll
+    for (int i = 0; i < MAX_CH; i++)
+        y[i] = i < ny ? (LEVEL0 ? cbar[i] : sbar[i]) : 0.0f;
+    A.y[A.site0[pl] + si] = make_float4(y[0], y[1], y[2], y[3]);
 }
 
 // The pixels whose bilinear footprint into an n1-wide plane can reach texel ti (src/solve_level1.cu:246-257).
@@ -173,6 +189,7 @@ __device__ __forceinline__ void reach(int ti, int n0, int n1, int& lo, int& hi)
 struct GatherArgs
 {
     const double* terms;
+    const float4* y;      // [site]: the site's sample of the other latent, from k_site_terms
     const double* mono;   // nmono matrices of c x c
     int nmono;
     long long site0[MAX_PLANES + 1];
@@ -227,6 +244,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
     for (int a = 0; a < MAX_CH; a++)
         g[a] = 0.0;
     const double* terms = A.terms + (size_t)A.site0[pl] * c;
+    const float4* ys = A.y + A.site0[pl];
 
     for (int py = py_lo; py <= py_hi; py++)
         for (int px = px_lo; px <= px_hi; px++)
@@ -274,28 +292,9 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
                 // the sample of the other latent at the site, and its monomials in a fixed layout: the constant,
                 // the four linear terms, then the ten products (i <= k) row by row; a narrower latent uses the
                 // entries whose indices are all below its channel count, which is the reference's order
-                float y[MAX_CH];
-                if (!LEVEL0)
-                {
-                    if (j == 0)
-                    {
-                        const size_t pi = (size_t)py * V.w0 + px;
-#pragma unroll
-                        for (int i = 0; i < MAX_CH; i++)
-                            if (i < c0)
-                                y[i] = __ldg(V.v0 + pi * c0 + i);
-                    }
-                    else
-                    {
-                        const Tap t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
-                        blend_u<MAX_CH>(V.v0, V.w0, c0, t0, y);
-                    }
-                }
-                else
-                {
-                    const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
-                    blend_u<MAX_CH>(V.v1, V.w1, c1, t1, y);
-                }
+                // (k_site_terms sampled it with the same taps and blend: the same floats)
+                const float4 y4 = __ldg(ys + (size_t)(py * V.w0 + px) * per + j);
+                const float y[MAX_CH] = { y4.x, y4.y, y4.z, y4.w };
                 const int ny_ = LEVEL0 ? c1 : c0;
                 if (slot == 0)
                 {
@@ -364,8 +363,8 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
         return (size_t)p.w0 * p.h0 * (size_t)(1 + k);
     });
     S.kc = k;
-    SiteArgs A{ d->weights, d->bias, d->cw, d->site_terms, {} };
-    GatherArgs G{ d->site_terms, d->mono[level0], nmono, {} };
+    SiteArgs A{ d->site_terms, (float4*)d->site_y, {} };
+    GatherArgs G{ d->site_terms, (const float4*)d->site_y, d->mono[level0], nmono, {} };
     long long at = 0;
     for (int i = 0; i < S.n; i++)
     {
@@ -374,10 +373,40 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     }
     A.site0[S.n] = G.site0[S.n] = at;
     const int sblocks = (int)(S.start[S.n] / SITE_THREADS);
-    if (level0)
-        k_site_terms<true><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A);
-    else
-        k_site_terms<false><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A);
+    SiteDecoder W{};
+    const int nin = d->nin, c0 = d->c0, c1 = d->c1;
+    for (int r = 0; r < d->nout; r++)
+    {
+        for (int q = 0; q < c1; q++)
+            W.w[r * 24 + q] = d->host_weights[(size_t)r * nin + q];
+        for (int i = 0; i < c0; i++)
+            W.w[r * 24 + 4 + i] = d->host_weights[(size_t)r * nin + c1 + i];
+        for (int i = 0; i < c0; i++)
+            for (int q = 0; q < c1; q++)
+                W.w[r * 24 + 8 + i * 4 + q] = d->host_weights[(size_t)r * nin + c1 + c0 + i * c1 + q];
+        W.b[r] = d->host_bias[r];
+        W.cw[r] = d->m.cw[r];
+    }
+#define NB_SITES(NO)                                                                                                  \
+    case NO:                                                                                                          \
+        if (level0)                                                                                                   \
+            k_site_terms<true, NO><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                                 \
+        else                                                                                                          \
+            k_site_terms<false, NO><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                                \
+        break;
+    switch (d->nout)
+    {
+        NB_SITES(3)
+        NB_SITES(6)
+        NB_SITES(9)
+        NB_SITES(12)
+        NB_SITES(15)
+        NB_SITES(18)
+    default:
+        set_error(NNTC_B200_ERR_STATE, "a material holds 1..6 RGB textures");
+        return NNTC_B200_ERR_STATE;
+    }
+#undef NB_SITES
     NB_LAUNCHED();
     dim3 grid((unsigned)(P_texels.start[P_texels.n] / GATHER_THREADS), SLOTS);
     if (level0)

@@ -166,10 +166,10 @@ __host__ __device__ __forceinline__ void subtexel(int kc, int j, int tx, int ty,
     float ox = 0.25f, oy = 0.25f;
     if (kc == 4)
     {
-        const float ax[4] = { -0.375f, -0.125f, 0.125f, 0.375f };
-        const float ay[4] = { -0.125f, 0.375f, -0.375f, 0.125f };
-        ox = ax[j];
-        oy = ay[j];
+        // the four offsets {(-3/8, -1/8), (-1/8, 3/8), (1/8, -3/8), (3/8, 1/8)}, selected rather than indexed so that
+        // a runtime j stays in registers
+        ox = j == 0 ? -0.375f : (j == 1 ? -0.125f : (j == 2 ? 0.125f : 0.375f));
+        oy = j == 0 ? -0.125f : (j == 1 ? 0.375f : (j == 2 ? -0.375f : 0.125f));
     }
     const int turns = (ty & 1) * 2 + (tx & 1);
     for (int r = 0; r < turns; r++)

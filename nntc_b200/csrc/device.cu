@@ -158,6 +158,8 @@ int upload_decoder(nntc_b200_device* d, const nntc_b200_model* m)
         return NNTC_B200_OK;
     NB_TRY(upload(d, d->weights, m->dec_w, (size_t)d->nout * d->nin * sizeof(float)));
     NB_TRY(upload(d, d->bias, m->dec_b, (size_t)d->nout * sizeof(float)));
+    std::memcpy(d->host_weights, m->dec_w, (size_t)d->nout * d->nin * sizeof(float));
+    std::memcpy(d->host_bias, m->dec_b, (size_t)d->nout * sizeof(float));
     return NNTC_B200_OK;
 }
 
@@ -559,6 +561,7 @@ int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain,
             sites += (size_t)p.w0 * p.h0 * 5;
         d->site_terms_count = sites * (size_t)std::max(m->c0, m->c1);
         NB_ALLOC(d->site_terms, d->site_terms_count * sizeof(double));
+        NB_ALLOC(d->site_y, sites * 4 * sizeof(float));
     }
     {
         // The objective's partials: one triple per 256-pixel block of every plane, then the three sums per plane.
@@ -615,7 +618,7 @@ void nntc_b200_device_destroy(nntc_b200_device* d)
     void* bufs[] = { d->weights, d->bias,     d->palette,   d->lo1,      d->hi1,         d->lo0,
                      d->hi0,     d->cw,       d->mono[0],   d->mono[1],  d->partial,     d->scalars,
                      d->counters, d->reduction, d->ls_partial, d->obj_partial, d->bc_stats, d->resid, d->site_terms,
-                     d->radix,
+                     d->site_y,    d->radix,
                      d->means,   d->cov,      d->hist,      d->scratch,  d->scratch8,    d->rgb8 };
     for (void* b : bufs)
         cudaFree(b);

@@ -92,6 +92,10 @@ struct nntc_b200_device
     std::vector<nb::DevPlane> planes;
     float* weights = nullptr;            // nout * nin
     float* bias = nullptr;               // nout
+    // Host copies of exactly what `weights` and `bias` hold (zero until a decoder is uploaded), for kernels that take
+    // the decoder as a launch parameter.
+    float host_weights[NNTC_B200_MAX_NOUT * NNTC_B200_MAX_NIN] = {};
+    float host_bias[NNTC_B200_MAX_NOUT] = {};
     float* palette = nullptr;            // MAX_CH * 16
     float* lo1 = nullptr;
     float* hi1 = nullptr;
@@ -109,6 +113,7 @@ struct nntc_b200_device
     unsigned int* radix = nullptr;       // 2 * MAX_CH * 2048 words: the grid fit's histograms and flags
     double* site_terms = nullptr;        // every site's gradient term of the assembly, max(C0, C1) per site at K = 4
     size_t site_terms_count = 0;         // doubles in site_terms
+    float* site_y = nullptr;             // every site's sample of the OTHER latent, 4 floats per site (assembly)
     int reference_shaped_assembly = 0;   // 1: the per-texel gather of the reference's shape (same bits, slower)
     float* resid = nullptr;              // the widest plane's residual, nout per pixel (init0 residual only)
     float* means = nullptr;              // the widest level-1 plane's block means, nout per texel

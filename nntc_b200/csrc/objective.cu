@@ -207,6 +207,115 @@ __global__ void __launch_bounds__(OBJ_THREADS) k_objective(Planes P, ObjArgs A)
     }
 }
 
+// The decoder as a launch parameter, in k_objective's fixed 24-slot row layout: with the row loop unrolled every
+// weight is an immediate constant-bank operand of its DFMA, so the dot products issue no shared-memory loads.
+struct ObjDecoder
+{
+    double w[MAX_NOUT * 24];
+    double b[MAX_NOUT];
+    double cw[MAX_NOUT];
+};
+
+// k_objective for a material of NOUT outputs (3 per texture), the decoder in the launch's parameters. The same sites,
+// the same operations in the same order, so the same bits as k_objective.
+template <int NOUT>
+__global__ void __launch_bounds__(OBJ_THREADS) k_objective_p(Planes P, ObjDecoder W, double* partial)
+{
+    __shared__ double red[32];
+    const int c0 = P.c0, c1 = P.c1, kc = P.kc;
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long local = base - P.start[pl] + threadIdx.x;
+    double weighted = 0.0, centre = 0.0, fractional = 0.0;
+    if (local < (long long)V.w0 * V.h0)
+    {
+        const int px = (int)(local % V.w0), py = (int)(local / V.w0);
+        for (int j = 0; j <= kc; j++)
+        {
+            float dx = 0.0f, dy = 0.0f;
+            if (j > 0)
+                subtexel(kc, j - 1, px, py, dx, dy);
+            const double u = ((double)px + 0.5 + (double)dx) / (double)V.w0;
+            const double v = ((double)py + 0.5 + (double)dy) / (double)V.h0;
+            double s[MAX_CH], c[MAX_CH];
+#pragma unroll
+            for (int q = 0; q < MAX_CH; q++)
+            {
+                s[q] = 0.0;
+                c[q] = 0.0;
+            }
+            obj_sample<MAX_CH>(V.v1, V.w1, V.h1, c1, u, v, c);
+            size_t ta = (size_t)local * NOUT, tb = ta, te = ta, tf = ta;
+            double w00 = 1.0, w10 = 0.0, w01 = 0.0, w11 = 0.0;
+            if (j == 0)
+            {
+#pragma unroll
+                for (int i = 0; i < MAX_CH; i++)
+                    if (i < c0)
+                        s[i] = (double)V.v0[local * c0 + i];
+            }
+            else
+            {
+                obj_sample<MAX_CH>(V.v0, V.w0, V.h0, c0, u, v, s);
+                const double x = u * (double)V.w0 - 0.5, y = v * (double)V.h0 - 0.5;
+                const double xf = floor(x), yf = floor(y);
+                const double fx = x - xf, fy = y - yf;
+                const int x0 = clampi((int)xf, V.w0), x1 = clampi((int)xf + 1, V.w0);
+                const int y0 = clampi((int)yf, V.h0), y1 = clampi((int)yf + 1, V.h0);
+                ta = ((size_t)y0 * V.w0 + x0) * NOUT;
+                tb = ((size_t)y0 * V.w0 + x1) * NOUT;
+                te = ((size_t)y1 * V.w0 + x0) * NOUT;
+                tf = ((size_t)y1 * V.w0 + x1) * NOUT;
+                w00 = (1.0 - fx) * (1.0 - fy);
+                w10 = fx * (1.0 - fy);
+                w01 = (1.0 - fx) * fy;
+                w11 = fx * fy;
+            }
+            double sc[16];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    sc[i * 4 + q] = s[i] * c[q];
+#pragma unroll
+            for (int r = 0; r < NOUT; r++)
+            {
+                const double t = j == 0 ? (double)__ldg(V.src + ta + r)
+                                        : w00 * (double)__ldg(V.src + ta + r) + w10 * (double)__ldg(V.src + tb + r) +
+                                              w01 * (double)__ldg(V.src + te + r) + w11 * (double)__ldg(V.src + tf + r);
+                const double* row = W.w + r * 24;
+                double acc = W.b[r];
+#pragma unroll
+                for (int h = 0; h < 4; h++)
+                    acc = fma(row[h], c[h], acc);
+#pragma unroll
+                for (int h = 0; h < 4; h++)
+                    acc = fma(row[4 + h], s[h], acc);
+#pragma unroll
+                for (int h = 0; h < 16; h++)
+                    acc = fma(row[8 + h], sc[h], acc);
+                const double e = acc - t;
+                weighted = fma(W.cw[r] * e, e, weighted);
+                if (j == 0)
+                    centre = fma(e, e, centre);
+                else
+                    fractional = fma(e, e, fractional);
+            }
+        }
+    }
+    const double a = block_sum(weighted, red);
+    const double b = block_sum(centre, red);
+    const double c = block_sum(fractional, red);
+    if (threadIdx.x == 0)
+    {
+        const size_t nb = gridDim.x;
+        partial[blockIdx.x] = a;
+        partial[nb + blockIdx.x] = b;
+        partial[2 * nb + blockIdx.x] = c;
+    }
+}
+
 // One block per plane: the plane's block partials added in a fixed order (a strided pass, then a fixed tree).
 __global__ void k_objective_reduce(Planes P, const double* partial, int nblocks, double* out)
 {
@@ -284,10 +393,41 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
     const int nblocks = (int)(P.start[P.n] / OBJ_THREADS);
     // device_create sized obj_partial for this layout: 3 doubles per pixel block, then 3 sums per plane.
     double* sums = d->obj_partial + (size_t)nblocks * 3;
-    ObjArgs A{ d->weights, d->bias, d->cw, d->obj_partial };
+    // the decoder as the device holds it, in the 24-slot row layout (a channel the layout does not use has weight 0)
+    ObjDecoder W{};
+    const int nin = d->nin, nout = d->nout, c0 = d->c0, c1 = d->c1;
+    for (int r = 0; r < nout; r++)
+    {
+        for (int slot = 0; slot < 24; slot++)
+        {
+            int col = -1;
+            if (slot < 4)
+                col = slot < c1 ? slot : -1;
+            else if (slot < 8)
+                col = slot - 4 < c0 ? c1 + slot - 4 : -1;
+            else
+            {
+                const int ii = (slot - 8) / 4, q = (slot - 8) % 4;
+                col = ii < c0 && q < c1 ? c1 + c0 + ii * c1 + q : -1;
+            }
+            W.w[r * 24 + slot] = col >= 0 ? (double)d->host_weights[(size_t)r * nin + col] : 0.0;
+        }
+        W.b[r] = (double)d->host_bias[r];
+        W.cw[r] = (double)d->m.cw[r];
+    }
     NB_TRY(block_begin(d));
     NB_TRY(ktimer_begin(d, NNTC_B200_K_OBJECTIVE));
-    k_objective<<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, A);
+    switch (nout)
+    {
+    case 3: k_objective_p<3><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 6: k_objective_p<6><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 9: k_objective_p<9><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 12: k_objective_p<12><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 15: k_objective_p<15><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 18: k_objective_p<18><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    default:
+        k_objective<<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, ObjArgs{ d->weights, d->bias, d->cw, d->obj_partial });
+    }
     NB_TRY(ktimer_end(d));
     NB_LAUNCHED();
     k_objective_reduce<<<P.n, 256, 0, d->stream>>>(P, d->obj_partial, nblocks, sums);
