@@ -12,9 +12,10 @@
 //     SITE computes it once, with the reference's arithmetic (rows in order, each column's sum over the rows in order,
 //     no contraction), into a per-site buffer of doubles; the gather then adds w_self * t_s exactly as the reference
 //     adds w_self * acc.
-//   - the stencil's monomial sums need only the site's sample of the OTHER latent (a bilinear blend of four texels) and
-//     the tap weights - a few dozen operations. They are gathered by one thread per (texel, slot): grid.y is the slot,
-//     so a warp shares one slot and its site range (the intersection of the two texels' footprints). Each slot's sums
+//   - the stencil's monomial sums need only the site's sample of the OTHER latent (a bilinear blend of four texels,
+//     which k_site_terms also stores per site) and the tap weights - a few dozen operations. They are gathered by one
+//     thread per (texel, slot): a block holds one slot, so a warp shares one slot and its site range (the
+//     intersection of the two texels' footprints). Each slot's sums
 //     receive the same terms in the same site order as the reference's, so every sum, and the expansion against the
 //     monomial matrices after it, is the same bits.
 //
@@ -200,8 +201,10 @@ struct GatherArgs
 template <bool LEVEL0>
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs A)
 {
-    const int slot = blockIdx.y;
-    const long long base = (long long)blockIdx.x * blockDim.x;
+    // the five slots of one range of texels are consecutive blocks, so they run side by side and share the range's
+    // sites in L2 (the sites of a neighbourhood are read by every slot of every texel they touch)
+    const int slot = (int)(blockIdx.x % SLOTS);
+    const long long base = (long long)(blockIdx.x / SLOTS) * blockDim.x;
     const int pl = plane_of(P, base);
     const PlaneView& V = P.p[pl];
     const long long ti = base - P.start[pl] + threadIdx.x;
@@ -215,12 +218,13 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
     slot_offset(slot, ox, oy);
     const int nbx = tx + ox, nby = ty + oy;
     const size_t T = (size_t)tw_ * th_;
+    const size_t sp = stencil_pos(tx, ty, tw_, th_);
     const int cc = c * c;
     if (nbx < 0 || nbx >= tw_ || nby >= th_)
     {
         // no neighbour in this direction: the reference's block is zero (no site touches both)
         for (int e = 0; e < cc; e++)
-            V.stencil[(size_t)(slot * cc + e) * T + ti] = 0.0;
+            V.stencil[(size_t)(slot * cc + e) * T + sp] = 0.0;
         return;
     }
     // the pixel range of sites that can touch both texels: the intersection of their footprints
@@ -345,7 +349,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
 #pragma unroll
     for (int e = 0; e < MAX_CH * MAX_CH; e++)
         if (e < cc)
-            V.stencil[(size_t)(slot * cc + e) * T + ti] = blk[e];
+            V.stencil[(size_t)(slot * cc + e) * T + sp] = blk[e];
     if (slot == 0)
     {
 #pragma unroll
@@ -408,7 +412,7 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     }
 #undef NB_SITES
     NB_LAUNCHED();
-    dim3 grid((unsigned)(P_texels.start[P_texels.n] / GATHER_THREADS), SLOTS);
+    const unsigned grid = (unsigned)(P_texels.start[P_texels.n] / GATHER_THREADS) * SLOTS;
     if (level0)
         k_gather<true><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
     else

@@ -250,6 +250,21 @@ __host__ __device__ __forceinline__ void slot_offset(int slot, int& dx, int& dy)
     dy = slot <= 1 ? 0 : 1;
 }
 
+// Where texel (x, y) of a w x h plane sits in the stencil's texel order. The order is colour-major: the four colours of
+// the quantised sweeps, (x & 1) + 2 (y & 1) in sweep order, one after another, each row-major. A sweep over one colour
+// then reads each of its stencil planes as one contiguous run instead of every other double, which halves the DRAM
+// sectors it touches; a row-major walk over all texels still reads two contiguous runs per warp.
+__host__ __device__ __forceinline__ size_t stencil_pos(int x, int y, int w, int h)
+{
+    const size_t w0c = (size_t)(w + 1) >> 1, w1c = (size_t)w >> 1;   // texels per row of x parity 0 / 1
+    const size_t h0c = (size_t)(h + 1) >> 1, h1c = (size_t)h >> 1;   // rows of y parity 0 / 1
+    const int cx = x & 1, cy = y & 1;
+    size_t base = cy ? (w0c + w1c) * h0c : 0;
+    if (cx)
+        base += cy ? w0c * h1c : w0c * h0c;
+    return base + (size_t)(y >> 1) * (cx ? w1c : w0c) + (size_t)(x >> 1);
+}
+
 __host__ __device__ __forceinline__ int slot_of(int dx, int dy)
 {
     for (int s = 0; s < SLOTS; s++)

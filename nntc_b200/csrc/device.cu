@@ -823,9 +823,13 @@ int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double
     {
         std::vector<double> soa(t * per);
         NB_TRY(download(d, soa.data(), w.stencil, soa.size() * sizeof(double)));
-        for (size_t e = 0; e < per; e++)
-            for (size_t i = 0; i < t; i++)
-                stencil[i * per + e] = soa[e * t + i];
+        // back from the colour-major SoA order to the reference's [texel][slot][i][j]
+        for (size_t i = 0; i < t; i++)
+        {
+            const size_t at = stencil_pos((int)(i % (size_t)w.w), (int)(i / (size_t)w.w), w.w, w.h);
+            for (size_t e = 0; e < per; e++)
+                stencil[i * per + e] = soa[e * t + at];
+        }
     }
     if (grad)
         NB_TRY(download(d, grad, w.grad, t * c * sizeof(double)));

@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
         const int px = gx * 4 + (t & 3), py = gy * 4 + (t >> 2);
         const bool in = px < w0 && py < h0;
         const size_t ti = in ? (size_t)py * w0 + px : 0;
+        const size_t sp = in ? stencil_pos(px, py, w0, h0) : 0;
         double acc = in ? B.grad[ti * C0 + i] : 0.0;
         for (int slot = 0; slot < SLOTS; slot++)
         {
@@ -366,12 +367,12 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
             const bool f_blk = lx >= 0 && lx < 4 && ly >= 0 && ly < 4;
             double* s_row = S + t * TS + slot * CC + i * C0;
             for (int j = 0; j < C0; j++)
-                s_row[j] = f_img && f_blk ? B.stencil[(size_t)(slot * CC + i * C0 + j) * T + ti] : 0.0;
+                s_row[j] = f_img && f_blk ? B.stencil[(size_t)(slot * CC + i * C0 + j) * T + sp] : 0.0;
             if (f_img && !f_blk)
             {
                 const double* xn = B.delta + ((size_t)fy * w0 + fx) * C0;
                 for (int j = 0; j < C0; j++)
-                    acc += B.stencil[(size_t)(slot * CC + i * C0 + j) * T + ti] * xn[j];
+                    acc += B.stencil[(size_t)(slot * CC + i * C0 + j) * T + sp] * xn[j];
             }
             if (slot == 0 || !in)
                 continue;
@@ -379,10 +380,10 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
             const int mx = ax - gx * 4, my = ay - gy * 4;
             if (ax < 0 || ax >= w0 || ay < 0 || ay >= h0 || (mx >= 0 && mx < 4 && my >= 0 && my < 4))
                 continue;
-            const size_t nt = (size_t)ay * w0 + ax;
+            const size_t nt = (size_t)ay * w0 + ax, np = stencil_pos(ax, ay, w0, h0);
             const double* xn = B.delta + nt * C0;
             for (int j = 0; j < C0; j++)
-                acc += B.stencil[(size_t)(slot * CC + j * C0 + i) * T + nt] * xn[j];
+                acc += B.stencil[(size_t)(slot * CC + j * C0 + i) * T + np] * xn[j];
         }
         a1[r] = acc;
         dv[r] = in ? (double)B.v0[ti * C0 + i] - (double)B.prev[ti * C0 + i] : 0.0;

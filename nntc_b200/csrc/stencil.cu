@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(Planes P, AsmArgs A)
                 blk[e] += s * __ldg(mat + e);
         }
         for (int e = 0; e < cc; e++)
-            V.stencil[(size_t)(slot * cc + e) * T + ti] = blk[e];
+            V.stencil[(size_t)(slot * cc + e) * T + stencil_pos(tx, ty, tw_, th_)] = blk[e];
     }
     for (int i = 0; i < c; i++)
         V.grad[ti * c + i] = g[i];
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(THREADS) k_diag(Planes P, Red R)
     if (t < (long long)T)
         for (int a = 0; a < c; a++)
         {
-            const double x = V.stencil[(size_t)(a * c + a) * T + t];
+            const double x = V.stencil[(size_t)(a * c + a) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)];
             v[0] += x;
             v[1] = x < v[1] ? x : v[1];
             v[2] = x > v[2] ? x : v[2];
@@ -468,40 +468,56 @@ __device__ __forceinline__ void apply_precond(const float* minv, const double* r
 
 // y_t = (H_tt + lambda I) x_t + sum of the owned slots' blocks times the forward neighbours + the transposes of the
 // backward neighbours' blocks (src/solve_level1.cu:781-828), in the reference's order of accumulation.
-__device__ __forceinline__ void stencil_apply(const PlaneView& V, int c, size_t T, long long t, double lambda,
-                                              const double* x, double* acc)
+template <int C>
+__device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long long t, double lambda, const double* x,
+                                              double* acc)
 {
+    constexpr int cc = C * C;
     const int tx = (int)(t % V.w), ty = (int)(t / V.w);
-    const int cc = c * c;
-    const double* xt = x + (size_t)t * c;
-    for (int i = 0; i < c; i++)
+    const size_t sp = stencil_pos(tx, ty, V.w, V.h);
+    const double* xt = x + (size_t)t * C;
+#pragma unroll
+    for (int i = 0; i < C; i++)
     {
         double s = lambda * xt[i];
-        for (int j = 0; j < c; j++)
-            s += V.stencil[(size_t)(i * c + j) * T + t] * xt[j];
+#pragma unroll
+        for (int j = 0; j < C; j++)
+            s += V.stencil[(size_t)(i * C + j) * T + sp] * xt[j];
         acc[i] = s;
     }
+    // Every neighbour's loads are issued whether or not the neighbour exists (from a clamped, in-range texel), and a
+    // missing neighbour's products are replaced by -0.0, which leaves any sum, a signed zero included, exactly as it
+    // was: the same bits as skipping those terms.
+#pragma unroll
     for (int slot = 1; slot < SLOTS; slot++)
     {
         int dx, dy;
         slot_offset(slot, dx, dy);
         const int fx = tx + dx, fy = ty + dy;
-        if (fx >= 0 && fx < V.w && fy >= 0 && fy < V.h)
-        {
-            const double* xn = x + ((size_t)fy * V.w + fx) * c;
-            for (int i = 0; i < c; i++)
-                for (int j = 0; j < c; j++)
-                    acc[i] += V.stencil[(size_t)(slot * cc + i * c + j) * T + t] * xn[j];
-        }
+        const bool fwd = fx >= 0 && fx < V.w && fy >= 0 && fy < V.h;
+        const int gx = fwd ? fx : tx, gy = fwd ? fy : ty;
+        const double* xn = x + ((size_t)gy * V.w + gx) * C;
+#pragma unroll
+        for (int i = 0; i < C; i++)
+#pragma unroll
+            for (int j = 0; j < C; j++)
+            {
+                const double e = V.stencil[(size_t)(slot * cc + i * C + j) * T + sp] * xn[j];
+                acc[i] += fwd ? e : -0.0;
+            }
         const int bx = tx - dx, by = ty - dy;
-        if (bx >= 0 && bx < V.w && by >= 0 && by < V.h)
-        {
-            const size_t nt = (size_t)by * V.w + bx;
-            const double* xn = x + nt * c;
-            for (int i = 0; i < c; i++)
-                for (int j = 0; j < c; j++)
-                    acc[i] += V.stencil[(size_t)(slot * cc + j * c + i) * T + nt] * xn[j];
-        }
+        const bool bwd = bx >= 0 && bx < V.w && by >= 0 && by < V.h;
+        const int hx = bwd ? bx : tx, hy = bwd ? by : ty;
+        const size_t nt = (size_t)hy * V.w + hx, np = stencil_pos(hx, hy, V.w, V.h);
+        const double* xb = x + nt * C;
+#pragma unroll
+        for (int i = 0; i < C; i++)
+#pragma unroll
+            for (int j = 0; j < C; j++)
+            {
+                const double e = V.stencil[(size_t)(slot * cc + j * C + i) * T + np] * xb[j];
+                acc[i] += bwd ? e : -0.0;
+            }
     }
 }
 
@@ -522,7 +538,8 @@ __global__ void __launch_bounds__(THREADS) k_precondition_init(Planes P, Red R)
         double a[MAX_CH * MAX_CH], inv[MAX_CH * MAX_CH];
         for (int i = 0; i < c; i++)
             for (int j = 0; j < c; j++)
-                a[i * c + j] = V.stencil[(size_t)(i * c + j) * T + t] + (i == j ? lambda : 0.0);
+                a[i * c + j] = V.stencil[(size_t)(i * c + j) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)] +
+                               (i == j ? lambda : 0.0);
         if (!invert(a, c, inv))
             for (int i = 0; i < c; i++)
                 for (int j = 0; j < c; j++)
@@ -575,6 +592,7 @@ __global__ void k_cg_start(Planes P, Red R)
     }
 }
 
+template <int C>
 __global__ void __launch_bounds__(THREADS) k_cg_matvec(Planes P, Red R)
 {
     __shared__ double sh[32];
@@ -586,13 +604,14 @@ __global__ void __launch_bounds__(THREADS) k_cg_matvec(Planes P, Red R)
     const PlaneView& V = P.p[pl];
     const long long t = base - P.start[pl] + threadIdx.x;
     const size_t T = (size_t)V.w * V.h;
-    const int c = P.c;
+    constexpr int c = C;
     double v[1] = { 0.0 };
     const int kind[1] = { 0 };
     if (t < (long long)T)
     {
         double acc[MAX_CH];
-        stencil_apply(V, c, T, t, s[S_LAMBDA], V.p, acc);
+        stencil_apply<C>(V, T, t, s[S_LAMBDA], V.p, acc);
+#pragma unroll
         for (int i = 0; i < c; i++)
         {
             V.ap[(size_t)t * c + i] = acc[i];
@@ -829,6 +848,7 @@ struct SweepArgs
     unsigned int* moved;   // [plane]
 };
 
+template <int C>
 __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
 {
     const long long base = (long long)blockIdx.x * blockDim.x;
@@ -841,46 +861,60 @@ __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
     const int tx = A.cx + 2 * (int)(ci % cwn);
     const int ty = A.cy + 2 * (int)(ci / cwn);
     const size_t t = (size_t)ty * V.w + tx;
+    const size_t sp = stencil_pos(tx, ty, V.w, V.h);
     const size_t T = (size_t)V.w * V.h;
-    const int c = P.c, cc = c * c;
+    constexpr int c = C, cc = C * C;
     const double lambda = A.scalars[(size_t)pl * S_COUNT + S_LAMBDA];
     double nb[MAX_CH];
+#pragma unroll
     for (int i = 0; i < c; i++)
         nb[i] = 0.0;
+    // as in stencil_apply: every load issued, a missing neighbour's products replaced by -0.0 (an exact no-op)
+#pragma unroll
     for (int slot = 1; slot < SLOTS; slot++)
     {
         int dx, dy;
         slot_offset(slot, dx, dy);
         const int fx = tx + dx, fy = ty + dy;
-        if (fx >= 0 && fx < V.w && fy >= 0 && fy < V.h)
-        {
-            const double* xn = V.x + ((size_t)fy * V.w + fx) * c;
-            for (int i = 0; i < c; i++)
-                for (int j = 0; j < c; j++)
-                    nb[i] += V.stencil[(size_t)(slot * cc + i * c + j) * T + t] * xn[j];
-        }
+        const bool fwd = fx >= 0 && fx < V.w && fy >= 0 && fy < V.h;
+        const int gx = fwd ? fx : tx, gy = fwd ? fy : ty;
+        const double* xn = V.x + ((size_t)gy * V.w + gx) * c;
+#pragma unroll
+        for (int i = 0; i < c; i++)
+#pragma unroll
+            for (int j = 0; j < c; j++)
+            {
+                const double e = V.stencil[(size_t)(slot * cc + i * c + j) * T + sp] * xn[j];
+                nb[i] += fwd ? e : -0.0;
+            }
         const int bx = tx - dx, by = ty - dy;
-        if (bx >= 0 && bx < V.w && by >= 0 && by < V.h)
-        {
-            const size_t nt = (size_t)by * V.w + bx;
-            const double* xn = V.x + nt * c;
-            for (int i = 0; i < c; i++)
-                for (int j = 0; j < c; j++)
-                    nb[i] += V.stencil[(size_t)(slot * cc + j * c + i) * T + nt] * xn[j];
-        }
+        const bool bwd = bx >= 0 && bx < V.w && by >= 0 && by < V.h;
+        const int hx = bwd ? bx : tx, hy = bwd ? by : ty;
+        const size_t nt = (size_t)hy * V.w + hx, np = stencil_pos(hx, hy, V.w, V.h);
+        const double* xb = V.x + nt * c;
+#pragma unroll
+        for (int i = 0; i < c; i++)
+#pragma unroll
+            for (int j = 0; j < c; j++)
+            {
+                const double e = V.stencil[(size_t)(slot * cc + j * c + i) * T + np] * xb[j];
+                nb[i] += bwd ? e : -0.0;
+            }
     }
     unsigned int changed = 0;
+#pragma unroll
     for (int q = 0; q < c; q++)
     {
         const size_t idx = t * c + q;
         const float l = A.lo[q], span = A.hi[q] - A.lo[q];
-        const double a = V.stencil[(size_t)(q * c + q) * T + t] + lambda;
+        const double a = V.stencil[(size_t)(q * c + q) * T + sp] + lambda;
         if (!(a > 0.0) || !(span > 0.0f))
             continue;
         double rest = nb[q];
+#pragma unroll
         for (int j = 0; j < c; j++)
             if (j != q)
-                rest += V.stencil[(size_t)(q * c + j) * T + t] * V.x[t * c + j];
+                rest += V.stencil[(size_t)(q * c + j) * T + sp] * V.x[t * c + j];
         const double b = V.grad[idx] + rest;
         const double want = (double)V.prev[idx] - b / a;
         const int kk = grid_index(l, A.hi[q], A.bits, (float)want);
@@ -1010,7 +1044,13 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     {
         NB_CUDA(cudaMemsetAsync(active + (it % CG_PROBE), 0, sizeof(unsigned int), d->stream));
         NB_TRY(ktimer_begin(d, NNTC_B200_K_MATVEC));
-        k_cg_matvec<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+        switch (P.c)
+        {
+        case 1: k_cg_matvec<1><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        case 2: k_cg_matvec<2><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        case 3: k_cg_matvec<3><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        default: k_cg_matvec<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        }
         NB_TRY(ktimer_end(d));
         NB_LAUNCHED();
         k_cg_alpha<<<P.n, 32, 0, d->stream>>>(P, R);
@@ -1091,7 +1131,14 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
                 continue;
             SweepArgs A{ d->scalars, level0 ? d->lo0 : d->lo1, level0 ? d->hi0 : d->hi1, bits, cx, cy, d->counters + CNT_SWEEP };
             NB_TRY(ktimer_begin(d, NNTC_B200_K_SWEEP));
-            k_quant_sweep<<<(int)(C.start[C.n] / THREADS), THREADS, 0, d->stream>>>(C, A);
+            const int sblocks = (int)(C.start[C.n] / THREADS);
+            switch (C.c)
+            {
+            case 1: k_quant_sweep<1><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
+            case 2: k_quant_sweep<2><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
+            case 3: k_quant_sweep<3><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
+            default: k_quant_sweep<4><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
+            }
             NB_TRY(ktimer_end(d));
             NB_LAUNCHED();
         }
