@@ -21,6 +21,8 @@
 //
 // Every plane of the chain is in each launch (nb::Planes); the per-site buffer holds every plane's sites.
 
+#include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "device.cuh"
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs 
 }
 
 // The pixels whose bilinear footprint into an n1-wide plane can reach texel ti (src/solve_level1.cu:246-257).
-__device__ __forceinline__ void reach(int ti, int n0, int n1, int& lo, int& hi)
+__host__ __device__ __forceinline__ void reach(int ti, int n0, int n1, int& lo, int& hi)
 {
     const double r = (double)n0 / (double)n1;
     lo = (int)ceil(((double)ti - 0.5) * r - 1.0);
@@ -187,17 +189,166 @@ __device__ __forceinline__ void reach(int ti, int n0, int n1, int& lo, int& hi)
     hi = hi > n0 - 1 ? n0 - 1 : hi;
 }
 
+// Whether site (px, py, j) touches both texel (tx, ty) and texel (nbx, nby) of the unknown latent (w x h, its pixels
+// w0 x h0), and with which weights. A merged tap's weight is the sum, in corner order, of the corner weights that
+// landed on that texel (src/solve_level1.cu:287-316, 466-498): accumulating the corners of the self texel and of the
+// neighbour from zero gives the same two weights.
+template <bool LEVEL0>
+__host__ __device__ __forceinline__ bool site_touches(int px, int py, int j, int kc, int tx, int ty, int nbx, int nby,
+                                                      int w0, int h0, int w, int h, float& w_self, float& w_other)
+{
+    float dx, dy;
+    site_offset(kc, j, px, py, dx, dy);
+    w_self = 0.0f;
+    w_other = 0.0f;
+    bool has_self = false, has_other = false;
+    if (LEVEL0 && j == 0)
+    {
+        has_self = px == tx && py == ty;
+        has_other = px == nbx && py == nby;
+        w_self = has_self ? 1.0f : 0.0f;
+        w_other = has_other ? 1.0f : 0.0f;
+    }
+    else
+    {
+        const Tap tq = tap_at(px, py, dx, dy, w0, h0, w, h);
+        float cw4[4];
+        tap_weights(tq, cw4);
+        const int cx4[4] = { tq.x0, tq.x1, tq.x0, tq.x1 };
+        const int cy4[4] = { tq.y0, tq.y0, tq.y1, tq.y1 };
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            if (cx4[q] == tx && cy4[q] == ty)
+            {
+                w_self += cw4[q];
+                has_self = true;
+            }
+            if (cx4[q] == nbx && cy4[q] == nby)
+            {
+                w_other += cw4[q];
+                has_other = true;
+            }
+        }
+    }
+    return has_self && has_other;
+}
+
+// ---- the gather's visit tables
+//
+// Away from the borders the sites that touch a texel and one of its neighbours, and their two weights, depend only on
+// where the texel sits relative to the pixel grid: for level 0 (the unknown at the pixels' own resolution, site
+// positions px + dx exact in float) on the texel's parity, which decides the subtexel rotation of its pixels; for
+// level 1 at exactly a quarter of a power-of-two plane (site positions ((px + 0.5 + dx) w) / w0 - 0.5 exact in
+// float) on nothing at all. So the visits are listed once, in the reference's site order, by running site_touches
+// on a texel in the middle of a plane of that shape, and every interior texel walks its list instead of testing
+// every site of its footprint; texels near a border, and planes of any other shape, take the full walk.
+
+constexpr int GATHER_CLASSES = 4;
+constexpr int GATHER_MARGIN = 3;   // texels this far from every border walk the table
+
+struct GatherTable
+{
+    int off[GATHER_CLASSES][SLOTS + 1];
+};
+
+// entry: x = (dpx + 64) | (dpy + 64) << 8 | j << 16, y = w_self bits, z = w_other bits; (dpx, dpy) relative to the
+// texel's first pixel (the texel itself at level 0, 4 tx / 4 ty at level 1)
+template <bool LEVEL0>
+static void build_gather_table(int kc, std::vector<int4>& tab, GatherTable& gt)
+{
+    tab.clear();
+    const int w = 64, h = 64, w0 = LEVEL0 ? 64 : 256, h0 = LEVEL0 ? 64 : 256, scale = LEVEL0 ? 1 : 4;
+    for (int cls = 0; cls < GATHER_CLASSES; cls++)
+    {
+        if (!LEVEL0 && cls > 0)
+        {
+            // level 1 has one class
+            for (int slot = 0; slot <= SLOTS; slot++)
+                gt.off[cls][slot] = gt.off[0][slot];
+            continue;
+        }
+        const int tx = 32 + (LEVEL0 ? (cls & 1) : 0), ty = 32 + (LEVEL0 ? (cls >> 1) : 0);
+        const int bx = tx * scale, by = ty * scale;
+        for (int slot = 0; slot < SLOTS; slot++)
+        {
+            gt.off[cls][slot] = (int)tab.size();
+            int ox, oy;
+            slot_offset(slot, ox, oy);
+            const int nbx = tx + ox, nby = ty + oy;
+            int px_lo, px_hi, py_lo, py_hi, qx_lo, qx_hi, qy_lo, qy_hi;
+            reach(tx, w0, w, px_lo, px_hi);
+            reach(ty, h0, h, py_lo, py_hi);
+            reach(nbx, w0, w, qx_lo, qx_hi);
+            reach(nby, h0, h, qy_lo, qy_hi);
+            px_lo = std::max(px_lo, qx_lo);
+            px_hi = std::min(px_hi, qx_hi);
+            py_lo = std::max(py_lo, qy_lo);
+            py_hi = std::min(py_hi, qy_hi);
+            for (int py = py_lo; py <= py_hi; py++)
+                for (int px = px_lo; px <= px_hi; px++)
+                    for (int j = 0; j <= kc; j++)
+                    {
+                        float ws, wo;
+                        if (!site_touches<LEVEL0>(px, py, j, kc, tx, ty, nbx, nby, w0, h0, w, h, ws, wo))
+                            continue;
+                        int4 e;
+                        e.x = (px - bx + 64) | (py - by + 64) << 8 | j << 16;
+                        std::memcpy(&e.y, &ws, sizeof(float));
+                        std::memcpy(&e.z, &wo, sizeof(float));
+                        e.w = 0;
+                        tab.push_back(e);
+                    }
+        }
+        gt.off[cls][SLOTS] = (int)tab.size();
+    }
+}
+
 struct GatherArgs
 {
     const double* terms;
     const float4* y;      // [site]: the site's sample of the other latent, from k_site_terms
     const double* mono;   // nmono matrices of c x c
+    const int4* tab;      // the visit tables of this level and K
+    GatherTable gt;
     int nmono;
+    unsigned tabled;      // bit i: plane i's interior texels may use the tables
     long long site0[MAX_PLANES + 1];
 };
 
+// The texel at position `pos` of the stencil's colour-major order (the inverse of stencil_pos).
+__device__ __forceinline__ void stencil_texel(long long pos, int w, int h, int& x, int& y)
+{
+    const long long w0c = (w + 1) >> 1, w1c = w >> 1, h0c = (h + 1) >> 1, h1c = h >> 1;
+    const long long n0 = w0c * h0c, n1 = w1c * h0c, n2 = w0c * h1c;
+    int cx = 0, cy = 0;
+    long long r = pos, rw = w0c;
+    if (r >= n0 + n1 + n2)
+    {
+        r -= n0 + n1 + n2;
+        cx = 1;
+        cy = 1;
+        rw = w1c;
+    }
+    else if (r >= n0 + n1)
+    {
+        r -= n0 + n1;
+        cy = 1;
+    }
+    else if (r >= n0)
+    {
+        r -= n0;
+        cx = 1;
+        rw = w1c;
+    }
+    x = 2 * (int)(r % rw) + cx;
+    y = 2 * (int)(r / rw) + cy;
+}
+
 // One thread per (texel, slot): the slot's monomial sums over every site that touches both the texel and the slot's
-// neighbour, in site order, expanded into the slot's block; the self-slot thread also gathers the gradient.
+// neighbour, in site order, expanded into the slot's block; the self-slot thread also gathers the gradient. Threads
+// take the texels in the stencil's colour-major order, so a warp's texels share a parity class (one visit table) and
+// its stores are contiguous.
 template <bool LEVEL0>
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs A)
 {
@@ -207,18 +358,19 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
     const long long base = (long long)(blockIdx.x / SLOTS) * blockDim.x;
     const int pl = plane_of(P, base);
     const PlaneView& V = P.p[pl];
-    const long long ti = base - P.start[pl] + threadIdx.x;
+    const long long sp = base - P.start[pl] + threadIdx.x;
     const int tw_ = V.w, th_ = V.h;
-    if (ti >= (long long)tw_ * th_)
+    if (sp >= (long long)tw_ * th_)
         return;
     const int c0 = P.c0, c1 = P.c1, kc = P.kc, per = 1 + kc, nmono = A.nmono;
     const int c = LEVEL0 ? c0 : c1;
-    const int tx = (int)(ti % tw_), ty = (int)(ti / tw_);
+    int tx, ty;
+    stencil_texel(sp, tw_, th_, tx, ty);
+    const size_t ti = (size_t)ty * tw_ + tx;
     int ox, oy;
     slot_offset(slot, ox, oy);
     const int nbx = tx + ox, nby = ty + oy;
     const size_t T = (size_t)tw_ * th_;
-    const size_t sp = stencil_pos(tx, ty, tw_, th_);
     const int cc = c * c;
     if (nbx < 0 || nbx >= tw_ || nby >= th_)
     {
@@ -227,17 +379,6 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
             V.stencil[(size_t)(slot * cc + e) * T + sp] = 0.0;
         return;
     }
-    // the pixel range of sites that can touch both texels: the intersection of their footprints
-    int px_lo, px_hi, py_lo, py_hi, qx_lo, qx_hi, qy_lo, qy_hi;
-    const int n1x = LEVEL0 ? V.w0 : V.w1, n1y = LEVEL0 ? V.h0 : V.h1;
-    reach(tx, V.w0, n1x, px_lo, px_hi);
-    reach(ty, V.h0, n1y, py_lo, py_hi);
-    reach(nbx, V.w0, n1x, qx_lo, qx_hi);
-    reach(nby, V.h0, n1y, qy_lo, qy_hi);
-    px_lo = max(px_lo, qx_lo);
-    px_hi = min(px_hi, qx_hi);
-    py_lo = max(py_lo, qy_lo);
-    py_hi = min(py_hi, qy_hi);
 
     double sums[MAX_MONO];
 #pragma unroll
@@ -249,86 +390,82 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
         g[a] = 0.0;
     const double* terms = A.terms + (size_t)A.site0[pl] * c;
     const float4* ys = A.y + A.site0[pl];
+    const int ny_ = LEVEL0 ? c1 : c0;
 
-    for (int py = py_lo; py <= py_hi; py++)
-        for (int px = px_lo; px <= px_hi; px++)
-            for (int j = 0; j <= kc; j++)
-            {
-                float dx, dy;
-                site_offset(kc, j, px, py, dx, dy);
-                // The site's taps on the unknown latent. A merged tap's weight is the sum, in corner order, of the
-                // corner weights that landed on that texel (src/solve_level1.cu:287-316, 466-498): accumulating the
-                // corners of the self texel and of the neighbour from zero gives the same two weights.
-                float w_self = 0.0f, w_other = 0.0f;
-                bool has_self = false, has_other = false;
-                if (LEVEL0 && j == 0)
-                {
-                    has_self = px == tx && py == ty;
-                    has_other = px == nbx && py == nby;
-                    w_self = has_self ? 1.0f : 0.0f;
-                    w_other = has_other ? 1.0f : 0.0f;
-                }
-                else
-                {
-                    const Tap tq = LEVEL0 ? tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0)
-                                          : tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
-                    float cw4[4];
-                    tap_weights(tq, cw4);
-                    const int cx4[4] = { tq.x0, tq.x1, tq.x0, tq.x1 };
-                    const int cy4[4] = { tq.y0, tq.y0, tq.y1, tq.y1 };
+    // one visit: the site's sample of the other latent (k_site_terms sampled it with the same taps and blend: the
+    // same floats) and its monomials in a fixed layout: the constant, the four linear terms, then the ten products
+    // (i <= k) row by row; a narrower latent uses the entries whose indices are all below its channel count, which is
+    // the reference's order
+    auto visit = [&](int px, int py, int j, float w_self, float w_other) {
+        const size_t site = (size_t)(py * V.w0 + px) * per + j;
+        const float4 y4 = __ldg(ys + site);
+        const float y[MAX_CH] = { y4.x, y4.y, y4.z, y4.w };
+        if (slot == 0)
+        {
+            const double* ts = terms + site * c;
 #pragma unroll
-                    for (int q = 0; q < 4; q++)
-                    {
-                        if (cx4[q] == tx && cy4[q] == ty)
-                        {
-                            w_self += cw4[q];
-                            has_self = true;
-                        }
-                        if (cx4[q] == nbx && cy4[q] == nby)
-                        {
-                            w_other += cw4[q];
-                            has_other = true;
-                        }
-                    }
-                }
-                if (!has_self || !has_other)
-                    continue;
-                // the sample of the other latent at the site, and its monomials in a fixed layout: the constant,
-                // the four linear terms, then the ten products (i <= k) row by row; a narrower latent uses the
-                // entries whose indices are all below its channel count, which is the reference's order
-                // (k_site_terms sampled it with the same taps and blend: the same floats)
-                const float4 y4 = __ldg(ys + (size_t)(py * V.w0 + px) * per + j);
-                const float y[MAX_CH] = { y4.x, y4.y, y4.z, y4.w };
-                const int ny_ = LEVEL0 ? c1 : c0;
-                if (slot == 0)
+            for (int a = 0; a < MAX_CH; a++)
+                if (a < c)
+                    g[a] += (double)w_self * ts[a];
+        }
+        const double scale = (double)w_self * (double)w_other;
+        sums[0] += scale * 1.0;
+#pragma unroll
+        for (int i = 0; i < MAX_CH; i++)
+            if (i < ny_)
+                sums[1 + i] += scale * (double)y[i];
+#pragma unroll
+        for (int p = 0; p < 10; p++)
+        {
+            const int i = pair_i(p), k2 = pair_k(p);
+            if (k2 < ny_)
+                sums[5 + p] += scale * ((double)y[i] * (double)y[k2]);
+        }
+    };
+
+    const bool interior = ((A.tabled >> pl) & 1u) && tx >= GATHER_MARGIN && tx < tw_ - GATHER_MARGIN &&
+                          ty >= GATHER_MARGIN && ty < th_ - GATHER_MARGIN;
+    if (interior)
+    {
+        const int cls = LEVEL0 ? (tx & 1) + 2 * (ty & 1) : 0;
+        const int bx = LEVEL0 ? tx : 4 * tx, by = LEVEL0 ? ty : 4 * ty;
+        const int e1 = A.gt.off[cls][slot + 1];
+        for (int e = A.gt.off[cls][slot]; e < e1; e++)
+        {
+            const int4 en = __ldg(A.tab + e);
+            visit(bx + (en.x & 0xff) - 64, by + ((en.x >> 8) & 0xff) - 64, en.x >> 16, __int_as_float(en.y),
+                  __int_as_float(en.z));
+        }
+    }
+    else
+    {
+        // the pixel range of sites that can touch both texels: the intersection of their footprints
+        int px_lo, px_hi, py_lo, py_hi, qx_lo, qx_hi, qy_lo, qy_hi;
+        const int n1x = LEVEL0 ? V.w0 : V.w1, n1y = LEVEL0 ? V.h0 : V.h1;
+        reach(tx, V.w0, n1x, px_lo, px_hi);
+        reach(ty, V.h0, n1y, py_lo, py_hi);
+        reach(nbx, V.w0, n1x, qx_lo, qx_hi);
+        reach(nby, V.h0, n1y, qy_lo, qy_hi);
+        px_lo = max(px_lo, qx_lo);
+        px_hi = min(px_hi, qx_hi);
+        py_lo = max(py_lo, qy_lo);
+        py_hi = min(py_hi, qy_hi);
+        for (int py = py_lo; py <= py_hi; py++)
+            for (int px = px_lo; px <= px_hi; px++)
+                for (int j = 0; j <= kc; j++)
                 {
-                    const double* ts = terms + ((size_t)(py * V.w0 + px) * per + j) * c;
-#pragma unroll
-                    for (int a = 0; a < MAX_CH; a++)
-                        if (a < c)
-                            g[a] += (double)w_self * ts[a];
+                    float ws, wo;
+                    if (site_touches<LEVEL0>(px, py, j, kc, tx, ty, nbx, nby, V.w0, V.h0, LEVEL0 ? V.w0 : V.w1,
+                                             LEVEL0 ? V.h0 : V.h1, ws, wo))
+                        visit(px, py, j, ws, wo);
                 }
-                const double scale = (double)w_self * (double)w_other;
-                sums[0] += scale * 1.0;
-#pragma unroll
-                for (int i = 0; i < MAX_CH; i++)
-                    if (i < ny_)
-                        sums[1 + i] += scale * (double)y[i];
-#pragma unroll
-                for (int p = 0; p < 10; p++)
-                {
-                    const int i = pair_i(p), k2 = pair_k(p);
-                    if (k2 < ny_)
-                        sums[5 + p] += scale * ((double)y[i] * (double)y[k2]);
-                }
-            }
+    }
 
     // the slot's block, expanded once against the monomial matrices in the reference's order (src/solve_level1.cu:382-399)
     double blk[MAX_CH * MAX_CH];
 #pragma unroll
     for (int e = 0; e < MAX_CH * MAX_CH; e++)
         blk[e] = 0.0;
-    const int ny_ = LEVEL0 ? c1 : c0;
     int q = 0;
 #pragma unroll
     for (int L = 0; L < MAX_MONO; L++)
@@ -368,7 +505,39 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     });
     S.kc = k;
     SiteArgs A{ d->site_terms, (float4*)d->site_y, {} };
-    GatherArgs G{ d->site_terms, (const float4*)d->site_y, d->mono[level0], nmono, {} };
+    GatherArgs G{};
+    G.terms = d->site_terms;
+    G.y = (const float4*)d->site_y;
+    G.mono = d->mono[level0];
+    G.nmono = nmono;
+    if (d->gtab_kc[level0] != k)
+    {
+        std::vector<int4> tab;
+        GatherTable gt{};
+        if (level0)
+            build_gather_table<true>(k, tab, gt);
+        else
+            build_gather_table<false>(k, tab, gt);
+        if (tab.size() > (size_t)GATHER_TABLE_MAX)
+        {
+            set_error(NNTC_B200_ERR_STATE, "the gather's visit table outgrew its buffer");
+            return NNTC_B200_ERR_STATE;
+        }
+        NB_TRY(upload(d, d->gtab[level0], tab.data(), tab.size() * sizeof(int4)));
+        static_assert(sizeof(d->gtab_off[0]) == sizeof(GatherTable), "visit table offsets");
+        std::memcpy(d->gtab_off[level0], &gt, sizeof(gt));
+        d->gtab_kc[level0] = k;
+    }
+    G.tab = (const int4*)d->gtab[level0];
+    std::memcpy(&G.gt, d->gtab_off[level0], sizeof(G.gt));
+    auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+    for (int i = 0; i < (int)d->planes.size(); i++)
+    {
+        const DevPlane& p = d->planes[(size_t)i];
+        const bool ok = level0 || (p.w0 == 4 * p.w1 && p.h0 == 4 * p.h1 && pow2(p.w1) && pow2(p.h1));
+        if (ok)
+            G.tabled |= 1u << i;
+    }
     long long at = 0;
     for (int i = 0; i < S.n; i++)
     {

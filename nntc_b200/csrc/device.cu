@@ -562,6 +562,8 @@ int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain,
         d->site_terms_count = sites * (size_t)std::max(m->c0, m->c1);
         NB_ALLOC(d->site_terms, d->site_terms_count * sizeof(double));
         NB_ALLOC(d->site_y, sites * 4 * sizeof(float));
+        NB_ALLOC(d->gtab[0], (size_t)GATHER_TABLE_MAX * 16);
+        NB_ALLOC(d->gtab[1], (size_t)GATHER_TABLE_MAX * 16);
     }
     {
         // The objective's partials: one triple per 256-pixel block of every plane, then the three sums per plane.
@@ -618,7 +620,7 @@ void nntc_b200_device_destroy(nntc_b200_device* d)
     void* bufs[] = { d->weights, d->bias,     d->palette,   d->lo1,      d->hi1,         d->lo0,
                      d->hi0,     d->cw,       d->mono[0],   d->mono[1],  d->partial,     d->scalars,
                      d->counters, d->reduction, d->ls_partial, d->obj_partial, d->bc_stats, d->resid, d->site_terms,
-                     d->site_y,    d->radix,
+                     d->site_y,    d->gtab[0],   d->gtab[1],  d->radix,
                      d->means,   d->cov,      d->hist,      d->scratch,  d->scratch8,    d->rgb8 };
     for (void* b : bufs)
         cudaFree(b);

@@ -47,6 +47,7 @@ enum Scalar
 constexpr int RGRID = 148 * 4;
 constexpr int RROWS = 3 + 2 * MAX_CH;
 constexpr int THREADS = 256;
+constexpr int GATHER_TABLE_MAX = 8192;   // int4 entries of one visit table
 // The counter words: the quantised sweeps' moved count per plane, block (c)'s four colour passes per plane, and the
 // conjugate gradients' active-plane counts of the last CG_PROBE iterations.
 constexpr int CNT_SWEEP = 0;
@@ -114,6 +115,9 @@ struct nntc_b200_device
     double* site_terms = nullptr;        // every site's gradient term of the assembly, max(C0, C1) per site at K = 4
     size_t site_terms_count = 0;         // doubles in site_terms
     float* site_y = nullptr;             // every site's sample of the OTHER latent, 4 floats per site (assembly)
+    void* gtab[2] = { nullptr, nullptr };// the gather's visit tables of level 1 / level 0 (GATHER_TABLE_MAX int4 each)
+    int gtab_kc[2] = { -1, -1 };         // the K each table was built for (-1: none yet)
+    int gtab_off[2][4][6] = {};          // each table's entry ranges per parity class and slot
     int reference_shaped_assembly = 0;   // 1: the per-texel gather of the reference's shape (same bits, slower)
     float* resid = nullptr;              // the widest plane's residual, nout per pixel (init0 residual only)
     float* means = nullptr;              // the widest level-1 plane's block means, nout per texel

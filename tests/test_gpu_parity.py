@@ -155,7 +155,11 @@ def random_state(mat, seed):
     return w, b, v0, v1
 
 
-@pytest.mark.parametrize("textures,c0,c1,w,h", SIZES)
+# power-of-two planes: level 1 at exactly a quarter, whose interior texels take the gather's visit tables
+POW2 = [(2, 4, 4, 64, 64), (1, 2, 3, 128, 64)]
+
+
+@pytest.mark.parametrize("textures,c0,c1,w,h", SIZES + POW2)
 def test_assembly_and_objective_vs_oracle(textures, c0, c1, w, h):
     mat = materials.small(21 + w, w, h, textures=textures, c0=c0, c1=c1)
     dw, db, v0, v1 = random_state(mat, w * h)
@@ -233,7 +237,7 @@ def test_bc_refine_vs_oracle(textures, c0, c1, w, h):
             assert np.array_equal(s.get_v0(i), v)
 
 
-@pytest.mark.parametrize("textures,c0,c1,w,h", [(4, 4, 4, 72, 40), (1, 3, 2, 45, 29)])
+@pytest.mark.parametrize("textures,c0,c1,w,h", [(4, 4, 4, 72, 40), (1, 3, 2, 45, 29)] + POW2)
 def test_assembly_shapes_agree_bit_for_bit(textures, c0, c1, w, h):
     """The per-site + per-(texel, slot) assembly and the reference-shaped per-texel gather give the same bits."""
     from nntc_b200 import lib
