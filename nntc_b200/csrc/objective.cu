@@ -278,24 +278,34 @@ __global__ void __launch_bounds__(OBJ_THREADS) k_objective_p(Planes P, ObjDecode
 #pragma unroll
                 for (int q = 0; q < 4; q++)
                     sc[i * 4 + q] = s[i] * c[q];
+            // every row's dot product advanced together, feature by feature (each row's own sum keeps phi's order),
+            // so that NOUT independent chains of DFMAs are in flight at once
+            double acc[NOUT];
+#pragma unroll
+            for (int r = 0; r < NOUT; r++)
+                acc[r] = W.b[r];
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+#pragma unroll
+                for (int r = 0; r < NOUT; r++)
+                    acc[r] = fma(W.w[r * 24 + h], c[h], acc[r]);
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+#pragma unroll
+                for (int r = 0; r < NOUT; r++)
+                    acc[r] = fma(W.w[r * 24 + 4 + h], s[h], acc[r]);
+#pragma unroll
+            for (int h = 0; h < 16; h++)
+#pragma unroll
+                for (int r = 0; r < NOUT; r++)
+                    acc[r] = fma(W.w[r * 24 + 8 + h], sc[h], acc[r]);
 #pragma unroll
             for (int r = 0; r < NOUT; r++)
             {
                 const double t = j == 0 ? (double)__ldg(V.src + ta + r)
                                         : w00 * (double)__ldg(V.src + ta + r) + w10 * (double)__ldg(V.src + tb + r) +
                                               w01 * (double)__ldg(V.src + te + r) + w11 * (double)__ldg(V.src + tf + r);
-                const double* row = W.w + r * 24;
-                double acc = W.b[r];
-#pragma unroll
-                for (int h = 0; h < 4; h++)
-                    acc = fma(row[h], c[h], acc);
-#pragma unroll
-                for (int h = 0; h < 4; h++)
-                    acc = fma(row[4 + h], s[h], acc);
-#pragma unroll
-                for (int h = 0; h < 16; h++)
-                    acc = fma(row[8 + h], sc[h], acc);
-                const double e = acc - t;
+                const double e = acc[r] - t;
                 weighted = fma(W.cw[r] * e, e, weighted);
                 if (j == 0)
                     centre = fma(e, e, centre);
