@@ -131,30 +131,48 @@ __global__ void k_block_means(const float* src, int w0, int h0, int nout, int w1
         means[i * (size_t)nout + c] = acc[c] * inv;
 }
 
-// Entry e < nout: the sum of channel e; entry nout + r nout + s: the sum of channel r times channel s. One block per
-// (stride, entry), one partial each, added by the host in block order.
+// Entry e < nout: the sum of channel e; entry nout + r nout + s: the sum of channel r times channel s. Block
+// (b, r) makes the partial b of the entries of channel r - its sum and its nout products - from ONE read of each row:
+// every entry's sum runs over the same texels in the same grid-stride order as one block per entry would, and is
+// folded by the same tree, so the partials do not depend on how entries share a block.
 __global__ void k_cov_partial(const float* v, size_t count, int nout, double* cov)
 {
     __shared__ double sh[256];
-    const int e = (int)blockIdx.y;
-    const int r = e < nout ? e : (e - nout) / nout;
-    const int s = e < nout ? -1 : (e - nout) % nout;
-    double acc = 0.0;
+    const int r = (int)blockIdx.y;
+    double acc[1 + MAX_NOUT];
+#pragma unroll
+    for (int q = 0; q <= MAX_NOUT; q++)
+        acc[q] = 0.0;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (size_t)gridDim.x * blockDim.x)
     {
-        const double a = (double)v[t * (size_t)nout + r];
-        acc += s < 0 ? a : a * (double)v[t * (size_t)nout + s];
+        const float* row = v + t * (size_t)nout;
+        const double a = (double)row[r];
+        acc[0] += a;
+#pragma unroll
+        for (int q = 0; q < MAX_NOUT; q++)
+            if (q < nout)
+                acc[1 + q] += a * (double)row[q];
     }
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int half = (int)blockDim.x / 2; half > 0; half >>= 1)
+#pragma unroll
+    for (int q = 0; q <= MAX_NOUT; q++)
     {
-        if ((int)threadIdx.x < half)
-            sh[threadIdx.x] += sh[threadIdx.x + half];
+        if (q > nout)
+            break;
         __syncthreads();
+        sh[threadIdx.x] = acc[q];
+        __syncthreads();
+        for (int half = (int)blockDim.x / 2; half > 0; half >>= 1)
+        {
+            if ((int)threadIdx.x < half)
+                sh[threadIdx.x] += sh[threadIdx.x + half];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+        {
+            const int e = q == 0 ? r : nout + r * nout + (q - 1);
+            cov[(size_t)e * COV_GRID + blockIdx.x] = sh[0];
+        }
     }
-    if (threadIdx.x == 0)
-        cov[(size_t)e * COV_GRID + blockIdx.x] = sh[0];
 }
 
 __global__ void k_quantise(const float* in, size_t n, int c, int bits, const float* lo, const float* hi, float* v,
@@ -349,7 +367,7 @@ static int cov_sums(nntc_b200_device* d, const float* rows, size_t count, int no
     const int entries = nout + nout * nout;
     if (!d->cov)
         NB_CUDA(cudaMalloc(&d->cov, (size_t)(MAX_NOUT + MAX_NOUT * MAX_NOUT) * COV_GRID * sizeof(double)));
-    dim3 grid((unsigned)COV_GRID, (unsigned)entries);
+    dim3 grid((unsigned)COV_GRID, (unsigned)nout);
     k_cov_partial<<<grid, 256, 0, d->stream>>>(rows, count, nout, d->cov);
     NB_LAUNCHED();
     std::vector<double> partial((size_t)entries * COV_GRID);
