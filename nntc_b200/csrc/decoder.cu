@@ -227,6 +227,169 @@ __global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape 
         }
 }
 
+// ---- the accumulation on the FP64 tensor cores
+//
+// Z = [phi (nin) | 1 | t (nout) | 0 ...] per site, 48 columns in six blocks of eight, and every product the normal
+// equations need is an entry of the 48 x 48 Gram Z^T Z: A from its upper-left mm x mm corner, the right-hand sides
+// from the columns after it. The 18 upper block pairs (I <= J, I < 4) of the Gram are accumulated with the FP64
+// tensor-core MMA (m8n8k4: an 8x4 slice of Z_I^T times a 4x8 slice of Z_J, four sites per step, every product exact
+// in double since both factors are floats). One block stages 128 sites' rows of Z; each of its four warps
+// takes 32 of them and keeps all 18 tiles in registers over all of its chunks; the warps' tiles are added in warp
+// order and each block writes one partial per entry, folded across blocks by k_ls_reduce in block order:
+// deterministic.
+
+constexpr int NE_THREADS = 128;
+constexpr int NE_WARPS = NE_THREADS / 32;
+constexpr int NE_STRIDE = 57;    // floats per staged site: 48 columns; an odd stride keeps the staging stores (one
+                                 // row per lane) conflict-free, and 57 = 25 (mod 32) spreads the four sites of one
+                                 // fragment load over the banks
+constexpr int NE_TILES = 18;     // block pairs I <= J of six blocks with I <= 3: the rows a < mm <= 25 the system
+                                 // reads (pairs of two target blocks are never needed)
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__host__ __device__ constexpr int tile_i(int t)
+{
+    return t < 6 ? 0 : (t < 11 ? 1 : (t < 15 ? 2 : (t < 18 ? 3 : (t < 20 ? 4 : 5))));
+}
+__host__ __device__ constexpr int tile_j(int t)
+{
+    return t < 6 ? t : (t < 11 ? t - 5 : (t < 15 ? t - 9 : (t < 18 ? t - 12 : (t < 20 ? t - 14 : 5))));
+}
+
+__global__ void __launch_bounds__(NE_THREADS, 4) k_ls_accumulate_mma(Planes P, LsArgs A)
+{
+    extern __shared__ double ne_sh[];
+    float* sz = (float*)ne_sh;   // [site][NE_STRIDE] floats; after the chunks, the warps' tiles as doubles
+    const int pl = blockIdx.y;
+    const PlaneView& V = P.p[pl];
+    const int c0 = P.c0, c1 = P.c1, nin = P.nin, nout = P.nout, kc = P.kc, mm = nin + 1;
+    const int per_pixel = 1 + kc;
+    const size_t sites = (size_t)V.w0 * V.h0 * per_pixel;
+    const size_t chunks = (sites + NE_THREADS - 1) / NE_THREADS;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double acc[NE_TILES][2];
+#pragma unroll
+    for (int t = 0; t < NE_TILES; t++)
+    {
+        acc[t][0] = 0.0;
+        acc[t][1] = 0.0;
+    }
+
+    for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
+    {
+        const size_t si = chunk * NE_THREADS + tid;
+        __syncthreads();   // the previous chunk's fragments have been read
+        float* row = sz + tid * NE_STRIDE;
+        // the site's row of Z with the solver's arithmetic (src/sample.cuh:154-178); a site outside the plane stages
+        // zeros
+        int q = 0;
+        if (si < sites)
+        {
+            const size_t pixel = si / (size_t)per_pixel;
+            const int j = (int)(si % (size_t)per_pixel);
+            const int px = (int)(pixel % (size_t)V.w0), py = (int)(pixel / (size_t)V.w0);
+            float dx, dy;
+            site_offset(kc, j, px, py, dx, dy);
+            float s[MAX_CH], c[MAX_CH];
+            const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
+            blend_u<MAX_CH>(V.v1, V.w1, c1, t1, c);
+            Tap t0{};
+            float w4[4];
+            if (j == 0)
+            {
+#pragma unroll
+                for (int i = 0; i < MAX_CH; i++)
+                    if (i < c0)
+                        s[i] = __ldg(V.v0 + pixel * c0 + i);
+            }
+            else
+            {
+                t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+                blend_u<MAX_CH>(V.v0, V.w0, c0, t0, s);
+                tap_weights(t0, w4);
+            }
+#pragma unroll
+            for (int jj = 0; jj < MAX_CH; jj++)
+                if (jj < c1)
+                    row[q++] = c[jj];
+#pragma unroll
+            for (int i = 0; i < MAX_CH; i++)
+                if (i < c0)
+                    row[q++] = s[i];
+#pragma unroll
+            for (int i = 0; i < MAX_CH; i++)
+#pragma unroll
+                for (int jj = 0; jj < MAX_CH; jj++)
+                    if (i < c0 && jj < c1)
+                        row[q++] = s[i] * c[jj];
+            row[q++] = 1.0f;
+            for (int r = 0; r < nout; r++)
+            {
+                float t;
+                if (j == 0)
+                    t = __ldg(V.src + pixel * nout + r);
+                else
+                    t = w4[0] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x0) * nout + r) +
+                        w4[1] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x1) * nout + r) +
+                        w4[2] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x0) * nout + r) +
+                        w4[3] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x1) * nout + r);
+                row[q++] = t;
+            }
+        }
+        for (; q < 48; q++)
+            row[q] = 0.0f;
+        __syncthreads();
+        // this warp's 32 sites, four per step
+        const float* base = sz + (size_t)(warp * 32 + (lane & 3)) * NE_STRIDE + (lane >> 2);
+#pragma unroll 2
+        for (int step = 0; step < 8; step++)
+        {
+            const float* f = base + (size_t)step * 4 * NE_STRIDE;
+            double frag[6];
+#pragma unroll
+            for (int b = 0; b < 6; b++)
+                frag[b] = (double)f[8 * b];
+#pragma unroll
+            for (int t = 0; t < NE_TILES; t++)
+                dmma_8x8x4(acc[t][0], acc[t][1], frag[tile_i(t)], frag[tile_j(t)]);
+        }
+    }
+
+    // the warps' tiles, added in warp order; each block writes the entries the system needs
+    __syncthreads();
+    double* red = ne_sh;   // [warp][tile][64]
+#pragma unroll
+    for (int t = 0; t < NE_TILES; t++)
+    {
+        const int r = lane >> 2, cidx = (lane & 3) * 2;
+        red[((size_t)warp * NE_TILES + t) * 64 + r * 8 + cidx] = acc[t][0];
+        red[((size_t)warp * NE_TILES + t) * 64 + r * 8 + cidx + 1] = acc[t][1];
+    }
+    __syncthreads();
+    for (int x = tid; x < NE_TILES * 64; x += NE_THREADS)
+    {
+        const int t = x / 64, r = (x % 64) / 8, cc = x % 8;
+        const int a = 8 * tile_i(t) + r, b = 8 * tile_j(t) + cc;
+        int e = -1;
+        if (a <= b && b < mm)
+            e = tri_index(a, b, mm);
+        else if (a < mm && b >= mm && b < mm + nout)
+            e = mm * (mm + 1) / 2 + (b - mm) * mm + a;   // rhs of output b - mm (t sits at column mm + c)
+        if (e < 0)
+            continue;
+        double sum = 0.0;
+        for (int w = 0; w < NE_WARPS; w++)
+            sum += red[((size_t)w * NE_TILES + t) * 64 + r * 8 + cc];
+        A.partial[((size_t)pl * A.entries + e) * LS_GRID + blockIdx.x] = sum;
+    }
+}
+
 __global__ void k_ls_reduce(const double* partial, int entries, int planes, const double* omega, double* out)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -258,11 +421,13 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     P.kc = k;
     NB_TRY(block_begin(d));
     dim3 grid(LS_GRID, (unsigned)P.n);
-    const size_t shared = LS_THREADS * sizeof(double) + (size_t)(S.nv + S.nt) * TILE * LS_STRIDE * sizeof(float);
-    NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
+    const size_t shared = std::max((size_t)NE_THREADS * NE_STRIDE * sizeof(float),
+                                   (size_t)NE_WARPS * NE_TILES * 64 * sizeof(double));
+    NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
     NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
-    k_ls_accumulate<<<grid, LS_THREADS, shared, d->stream>>>(P, S, LsArgs{ d->ls_partial, entries });
+    k_ls_accumulate_mma<<<grid, NE_THREADS, shared, d->stream>>>(P, LsArgs{ d->ls_partial, entries });
     NB_TRY(ktimer_end(d));
+    (void)S;
     NB_LAUNCHED();
     k_ls_reduce<<<grid_for((size_t)entries, 128), 128, 0, d->stream>>>(d->ls_partial, entries, P.n, omega,
                                                                       d->reduction);
