@@ -314,6 +314,7 @@ struct GatherArgs
     int nmono;
     unsigned tabled;      // bit i: plane i's interior texels may use the tables
     long long site0[MAX_PLANES + 1];
+    long long bstart[MAX_PLANES + 1];   // each plane's first block
 };
 
 // The texel at position `pos` of the stencil's colour-major order (the inverse of stencil_pos).
@@ -352,16 +353,27 @@ __device__ __forceinline__ void stencil_texel(long long pos, int w, int h, int& 
 template <bool LEVEL0>
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs A)
 {
-    // the five slots of one range of texels are consecutive blocks, so they run side by side and share the range's
-    // sites in L2 (the sites of a neighbourhood are read by every slot of every texel they touch)
-    const int slot = (int)(blockIdx.x % SLOTS);
-    const long long base = (long long)(blockIdx.x / SLOTS) * blockDim.x;
-    const int pl = plane_of(P, base);
+    // Block order: (region, colour, slot) with the slot fastest. The five slots of one run of texels, and the four
+    // colours of one region of the plane, are consecutive blocks, so they run side by side and share the region's sites
+    // in L2: every slot of every texel that a site touches reads it, and the texels of one colour alone already touch
+    // every site of their region.
+    int pl = 0;
+    while (pl + 1 < P.n && A.bstart[pl + 1] <= (long long)blockIdx.x)
+        pl++;
+    const long long lb = (long long)blockIdx.x - A.bstart[pl];
+    const int slot = (int)(lb % SLOTS);
+    const int colour = (int)((lb / SLOTS) % 4);
+    const long long region = lb / SLOTS / 4;
     const PlaneView& V = P.p[pl];
-    const long long sp = base - P.start[pl] + threadIdx.x;
     const int tw_ = V.w, th_ = V.h;
-    if (sp >= (long long)tw_ * th_)
+    const long long w0c = (tw_ + 1) >> 1, w1c = tw_ >> 1, h0c = (th_ + 1) >> 1, h1c = th_ >> 1;
+    const long long ncol[4] = { w0c * h0c, w1c * h0c, w0c * h1c, w1c * h1c };
+    const long long within = region * GATHER_THREADS + threadIdx.x;
+    if (within >= ncol[colour])
         return;
+    long long sp = within;   // the texel's place in the stencil's colour-major order
+    for (int q = 0; q < colour; q++)
+        sp += ncol[q];
     const int c0 = P.c0, c1 = P.c1, kc = P.kc, per = 1 + kc, nmono = A.nmono;
     const int c = LEVEL0 ? c0 : c1;
     int tx, ty;
@@ -581,7 +593,16 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     }
 #undef NB_SITES
     NB_LAUNCHED();
-    const unsigned grid = (unsigned)(P_texels.start[P_texels.n] / GATHER_THREADS) * SLOTS;
+    long long blocks = 0;
+    for (int i = 0; i < P_texels.n; i++)
+    {
+        G.bstart[i] = blocks;
+        const PlaneView& v = P_texels.p[i];
+        const long long largest = (long long)((v.w + 1) / 2) * ((v.h + 1) / 2);   // colour 0
+        blocks += (largest + GATHER_THREADS - 1) / GATHER_THREADS * 4 * SLOTS;
+    }
+    G.bstart[P_texels.n] = blocks;
+    const unsigned grid = (unsigned)blocks;
     if (level0)
         k_gather<true><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
     else
