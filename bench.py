@@ -42,7 +42,6 @@ sys.path.insert(0, ROOT)
 
 from nntc_b200 import abi, check, lib, materials  # noqa: E402
 
-# Per-unit figures of the dominant kernels (DESIGN.md states their derivation): bytes a launch must move at least.
 CONFIG_NAMES = {0: "1x256x256 noise+rects c0=2 c1=4", 1: "4x512x512 pbr c0=2 c1=4", 2: "4x1024x1024 pbr c0=2 c1=4",
                 3: "4x2048x1024 pbr c0=4 c1=4", 4: "6x4096x4096 pbr c0=4 c1=4"}
 
@@ -315,6 +314,29 @@ def main():
     return 0
 
 
+# DRAM bytes (read + write) per launch of each timed kernel group, per level-0 pixel of the chain (per level-1 texel for
+# the CG matvec), from one ncu capture (--set full) of the 4 x 2048 x 1024 material; a launch's traffic grows with the
+# pixels it covers, so the bench scales these to its own workload.
+TRAFFIC_PER_UNIT = {
+    "assemble_level0": (843234000 + 2507003000) / 2796160,   # k_site_terms<1> + k_gather<1>
+    "assemble_level1": (842598000 + 1440221000) / 2796160,   # k_site_terms<0> + k_gather<0>
+    "objective": 186502656 / 2796160,
+    "normal_equations": 197941504 / 2796160,
+    "bc_refine": 1194571624 / 2796160,                       # one colour
+}
+
+# What bounds each group, from the same captures: the roofline the HBM fraction alone does not show.
+BINDING = {
+    "assemble_level0": "FP32/ALU issue (site terms, ~80% issue) and L2 latency (gather); FP64 compute, not HBM",
+    "assemble_level1": "FP32/ALU issue (site terms) and L2 latency (gather); FP64 compute, not HBM",
+    "objective": "FP64 pipe (~50% of peak)",
+    "normal_equations": "FP64 tensor pipe and site staging",
+    "bc_refine": "latency of 128 ordered selector steps per block",
+    "quant_sweep": "HBM (level-0 colour launch ~79% of measured copy bandwidth)",
+    "cg_matvec": "HBM",
+}
+
+
 def roofline(name, stat, mat, hbm, tf, src):
     """The dominant kernel against the HBM roofline: its algorithmic bytes per launch over its mean launch time."""
     launches, ms = stat
@@ -322,13 +344,17 @@ def roofline(name, stat, mat, hbm, tf, src):
         return None
     per = algorithmic_bytes(name, mat)
     achieved = per / (ms / launches / 1000.0) / 1e9
+    t0 = sum(p[0] * p[1] for p in mat.planes)
+    traffic = round(TRAFFIC_PER_UNIT[name] * t0) if name in TRAFFIC_PER_UNIT else None
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
-            "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": src,
-            "bytes_per_launch": per, "launches": launches, "ms_per_launch": round(ms / launches, 4)}
+            "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": src,
+            "traffic_source": "ncu DRAM bytes of the 4x2048x1024 workload scaled by level-0 pixels" if traffic else None,
+            "binding": BINDING.get(name), "bytes_per_launch": per, "launches": launches,
+            "ms_per_launch": round(ms / launches, 4)}
 
 
 def algorithmic_bytes(name, mat):
-    """Bytes a launch must read and write at least (every plane of the chain), the figures DESIGN.md derives."""
+    """Bytes a launch must read and write at least (every plane of the chain): its inputs once and its outputs once."""
     c0, c1, nout = mat.c0, mat.c1, 3 * len(mat.textures)
     t0 = sum(p[0] * p[1] for p in mat.planes)
     t1 = sum(p[2] * p[3] for p in mat.planes)

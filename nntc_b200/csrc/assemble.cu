@@ -367,13 +367,13 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
     const PlaneView& V = P.p[pl];
     const int tw_ = V.w, th_ = V.h;
     const long long w0c = (tw_ + 1) >> 1, w1c = tw_ >> 1, h0c = (th_ + 1) >> 1, h1c = th_ >> 1;
-    const long long ncol[4] = { w0c * h0c, w1c * h0c, w0c * h1c, w1c * h1c };
+    const long long n0 = w0c * h0c, n1 = w1c * h0c, n2 = w0c * h1c, n3 = w1c * h1c;
+    const long long ncol = colour == 0 ? n0 : (colour == 1 ? n1 : (colour == 2 ? n2 : n3));
     const long long within = region * GATHER_THREADS + threadIdx.x;
-    if (within >= ncol[colour])
+    if (within >= ncol)
         return;
-    long long sp = within;   // the texel's place in the stencil's colour-major order
-    for (int q = 0; q < colour; q++)
-        sp += ncol[q];
+    // the texel's place in the stencil's colour-major order
+    const long long sp = within + (colour == 0 ? 0 : (colour == 1 ? n0 : (colour == 2 ? n0 + n1 : n0 + n1 + n2)));
     const int c0 = P.c0, c1 = P.c1, kc = P.kc, per = 1 + kc, nmono = A.nmono;
     const int c = LEVEL0 ? c0 : c1;
     int tx, ty;
