@@ -64,7 +64,7 @@ struct SiteDecoder
 };
 
 template <bool LEVEL0, int NOUT>
-__global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, SiteArgs A, SiteDecoder W)
+__global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __grid_constant__ SiteArgs A, SiteDecoder W)
 {
     const long long base = (long long)blockIdx.x * blockDim.x;
     const int pl = plane_of(P, base);

@@ -638,6 +638,7 @@ __global__ void k_cg_alpha(Planes P, Red R)
     }
 }
 
+template <int C>
 __global__ void __launch_bounds__(THREADS) k_cg_update(Planes P, Red R)
 {
     __shared__ double sh[2 * 32];
@@ -649,13 +650,14 @@ __global__ void __launch_bounds__(THREADS) k_cg_update(Planes P, Red R)
     const PlaneView& V = P.p[pl];
     const long long t = base - P.start[pl] + threadIdx.x;
     const size_t T = (size_t)V.w * V.h;
-    const int c = P.c;
+    constexpr int c = C;   // the channel count as a constant: r, z and the preconditioner stay in registers
     double v[2] = { 0.0, 0.0 };
     const int kind[2] = { 0, 0 };
     if (t < (long long)T)
     {
         const double alpha = s[S_ALPHA];
         double r[MAX_CH], z[MAX_CH];
+#pragma unroll
         for (int i = 0; i < c; i++)
         {
             const size_t q = (size_t)t * c + i;
@@ -664,9 +666,19 @@ __global__ void __launch_bounds__(THREADS) k_cg_update(Planes P, Red R)
             V.r[q] = r[i];
         }
         float minv[MAX_CH * MAX_CH];
+#pragma unroll
         for (int i = 0; i < c * c; i++)
             minv[i] = V.precond[(size_t)t * c * c + i];
-        apply_precond(minv, r, c, z);
+#pragma unroll
+        for (int i = 0; i < c; i++)
+        {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < c; j++)
+                acc += (double)minv[i * c + j] * r[j];
+            z[i] = acc;
+        }
+#pragma unroll
         for (int i = 0; i < c; i++)
         {
             V.z[(size_t)t * c + i] = z[i];
@@ -1055,7 +1067,13 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
         NB_LAUNCHED();
         k_cg_alpha<<<P.n, 32, 0, d->stream>>>(P, R);
         NB_LAUNCHED();
-        k_cg_update<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+        switch (P.c)
+        {
+        case 1: k_cg_update<1><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        case 2: k_cg_update<2><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        case 3: k_cg_update<3><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        default: k_cg_update<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+        }
         NB_LAUNCHED();
         k_cg_beta<<<P.n, 32, 0, d->stream>>>(P, R, it, active + (it % CG_PROBE));
         NB_LAUNCHED();
