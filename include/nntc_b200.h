@@ -149,6 +149,11 @@ int nntc_b200_abi_sizes(size_t* out, int n);
 /* ---- lifecycle: src/init.cu:76-382 (device_select, device_create, device_destroy, device_memory) ---- */
 int nntc_b200_device_select(int index, nntc_b200_device_info* info);           /* returns 1 if usable */
 int nntc_b200_device_create(const nntc_b200_model* m, const float* const* source_chain, nntc_b200_device** out);
+/* The same device model from the base plane alone (w0[0] x h0[0] x nout floats): the other levels of the default
+ * source chain - each the 2x2 box of the one above, src/mips.cpp:80-84 over src/image.h:343-364 - are built on the
+ * device, bit for bit the reference's. The model's planes must be that chain's sizes (each the floor halving of the
+ * one above, never below one texel). */
+int nntc_b200_device_create_from_base(const nntc_b200_model* m, const float* base, nntc_b200_device** out);
 void nntc_b200_device_destroy(nntc_b200_device* d);                             /* NULL is a no-op */
 size_t nntc_b200_device_memory(const nntc_b200_device* d);
 
@@ -322,6 +327,7 @@ int nntc_b200_probe_normal_equations(nntc_b200_device* d, double* out, size_t n)
 int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double* stencil, double* grad,
                               float* precond, double* cg_x, float* prev);
 int nntc_b200_probe_monomials(nntc_b200_device* d, int level0, double* out, size_t n);
+int nntc_b200_probe_source(nntc_b200_device* d, int plane, float* out, size_t n);   /* plane's source, HWC */
 
 #ifdef __cplusplus
 }

@@ -33,6 +33,7 @@ PROTOTYPES = {
     "nntc_b200_abi_sizes": (_I, [C.POINTER(_S), _I]),
     "nntc_b200_device_select": (_I, [_I, C.POINTER(abi.DeviceInfo)]),
     "nntc_b200_device_create": (_I, [_M, _PPF, C.POINTER(_P)]),
+    "nntc_b200_device_create_from_base": (_I, [_M, _PF, C.POINTER(_P)]),
     "nntc_b200_device_destroy": (None, [_P]),
     "nntc_b200_device_memory": (_S, [_P]),
     "nntc_b200_init_level0": (_I, [_P, _M, _PF, _I, _PPU8]),
@@ -83,6 +84,7 @@ PROTOTYPES = {
     "nntc_b200_probe_normal_equations": (_I, [_P, _PD, _S]),
     "nntc_b200_probe_workspace": (_I, [_P, _I, _I, _PD, _PD, _PF, _PD, _PF]),
     "nntc_b200_probe_monomials": (_I, [_P, _I, _PD, _S]),
+    "nntc_b200_probe_source": (_I, [_P, _I, _PF, _S]),
 }
 
 

@@ -265,6 +265,12 @@ __host__ __device__ __forceinline__ size_t stencil_pos(int x, int y, int w, int 
     return base + (size_t)(y >> 1) * (cx ? w1c : w0c) + (size_t)(x >> 1);
 }
 
+// The floor halving of a mip chain, never below one texel (src/image.h:335-338).
+__host__ __device__ __forceinline__ int mip_dim(int n)
+{
+    return n / 2 > 0 ? n / 2 : 1;
+}
+
 __host__ __device__ __forceinline__ int slot_of(int dx, int dy)
 {
     for (int s = 0; s < SLOTS; s++)

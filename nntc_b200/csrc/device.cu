@@ -431,7 +431,14 @@ int nntc_b200_device_select(int index, nntc_b200_device_info* info)
     return 1;
 }
 
-int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain, nntc_b200_device** out)
+static int refuse_arg(const std::string& why)
+{
+    nb::set_error(NNTC_B200_ERR_ARG, why);
+    return NNTC_B200_ERR_ARG;
+}
+
+// The device model; a null chain[i] leaves plane i's source to the caller (the from-base path fills it on the device).
+static int device_create_impl(const nntc_b200_model* m, const float* const* chain, nntc_b200_device** out)
 {
     *out = nullptr;
     NB_TRY(validate(m));
@@ -482,7 +489,8 @@ int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain,
         NB_ALLOC(p.v1, n1 * m->c1 * sizeof(float));
         NB_ALLOC(p.k0, n0 * m->c0);
         NB_ALLOC(p.k1, n1 * m->c1);
-        NB_CK(cudaMemcpy(p.src, chain[i], n0 * m->nout * sizeof(float), cudaMemcpyHostToDevice));
+        if (chain[i])
+            NB_CK(cudaMemcpy(p.src, chain[i], n0 * m->nout * sizeof(float), cudaMemcpyHostToDevice));
         NB_CK(cudaMemset(p.v0, 0, n0 * m->c0 * sizeof(float)));
         NB_CK(cudaMemset(p.v1, 0, n1 * m->c1 * sizeof(float)));
         NB_CK(cudaMemset(p.k0, 0, n0 * m->c0));
@@ -582,11 +590,47 @@ int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain,
         NB_ALLOC(d->resid, max0 * m->nout * sizeof(float));
     NB_CK(cudaMallocHost(&d->host_scalars, (size_t)MAX_PLANES * S_COUNT * sizeof(double)));
     NB_CK(cudaMallocHost(&d->host_counters, (size_t)COUNTERS * sizeof(unsigned int)));
+    // the set-up's copies and clears went to the legacy stream; the model's own stream does not wait for it
+    NB_CK(cudaDeviceSynchronize());
     d->m.has_decoder = 0;
 #undef NB_ALLOC
 #undef NB_CK
     *out = d;
     return NNTC_B200_OK;
+}
+
+int nntc_b200_device_create(const nntc_b200_model* m, const float* const* chain, nntc_b200_device** out)
+{
+    *out = nullptr;
+    NB_TRY(validate(m));
+    if (!chain)
+        return refuse_arg("the source chain is null");
+    for (int i = 0; i < m->nplanes; i++)
+        if (!chain[i])
+            return refuse_arg("plane " + std::to_string(i) + " of the source chain is null");
+    return device_create_impl(m, chain, out);
+}
+
+int nntc_b200_device_create_from_base(const nntc_b200_model* m, const float* base, nntc_b200_device** out)
+{
+    *out = nullptr;
+    NB_TRY(validate(m));
+    if (!base)
+        return refuse_arg("the base plane is null");
+    // the chain must be the default one: every level the floor halving of the one above, never below one texel
+    for (int i = 1; i < m->nplanes; i++)
+        if (m->w0[i] != nb::mip_dim(m->w0[i - 1]) || m->h0[i] != nb::mip_dim(m->h0[i - 1]))
+            return refuse_arg("plane " + std::to_string(i) + " is not the box halving of plane " + std::to_string(i - 1));
+    std::vector<const float*> chain((size_t)m->nplanes, nullptr);
+    chain[0] = base;
+    NB_TRY(device_create_impl(m, chain.data(), out));
+    const int st = nb::build_source_chain(*out);
+    if (st != NNTC_B200_OK)
+    {
+        nntc_b200_device_destroy(*out);
+        *out = nullptr;
+    }
+    return st;
 }
 
 void nntc_b200_device_destroy(nntc_b200_device* d)
@@ -842,6 +886,19 @@ int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double
     if (prev)
         NB_TRY(download(d, prev, w.prev, t * c * sizeof(float)));
     return NNTC_B200_OK;
+}
+
+int nntc_b200_probe_source(nntc_b200_device* d, int plane, float* out, size_t n)
+{
+    NB_TRY(check_plane(d, plane));
+    const DevPlane& p = d->planes[(size_t)plane];
+    const size_t want = (size_t)p.w0 * p.h0 * d->nout;
+    if (n < want)
+    {
+        set_error(NNTC_B200_ERR_ARG, "source buffer too small");
+        return NNTC_B200_ERR_ARG;
+    }
+    return download(d, out, p.src, want * sizeof(float));
 }
 
 int nntc_b200_probe_monomials(nntc_b200_device* d, int level0, double* out, size_t n)

@@ -209,6 +209,9 @@ int ktimer_begin(nntc_b200_device* d, int kind);
 int ktimer_end(nntc_b200_device* d);
 int ktimer_harvest(nntc_b200_device* d);
 
+// Planes 1.. of the source chain from plane 0, on the device: each level the 2x2 box of the one above.
+int build_source_chain(nntc_b200_device* d);
+
 // Upload on the model's stream and wait (the staging buffer is the caller's).
 int upload(nntc_b200_device* d, void* dst, const void* src, size_t bytes);
 int download(nntc_b200_device* d, void* dst, const void* src, size_t bytes);

@@ -13,14 +13,20 @@ from . import abi, check, lib
 
 
 class Session:
-    def __init__(self, material, model: abi.Model | None = None):
+    def __init__(self, material, model: abi.Model | None = None, from_base: bool = False):
+        """from_base: upload the base plane only and build the rest of the source chain on the device."""
         self.material = material
         self.m = model if model is not None else abi.make_model(material)
         self._chain = [np.ascontiguousarray(c, np.float32) for c in material.chain]
         self.per_site = (C.c_double * len(material.per_site))(*material.per_site)
         handle = C.c_void_p()
-        check(lib().nntc_b200_device_create(C.byref(self.m), abi.float_ptrs(self._chain), C.byref(handle)),
-              "device_create")
+        if from_base:
+            base = self._chain[0].ravel()
+            check(lib().nntc_b200_device_create_from_base(C.byref(self.m), base.ctypes.data_as(C.POINTER(C.c_float)),
+                                                           C.byref(handle)), "device_create_from_base")
+        else:
+            check(lib().nntc_b200_device_create(C.byref(self.m), abi.float_ptrs(self._chain), C.byref(handle)),
+                  "device_create")
         self.d = handle
 
     def close(self):
@@ -44,6 +50,11 @@ class Session:
     def u8_planes(self, level):
         c = self.m.c0 if level == 0 else self.m.c1
         return [np.zeros((self.n0(i) if level == 0 else self.n1(i)) * c, np.uint8) for i in range(self.m.nplanes)]
+
+    def get_source(self, i):
+        a = np.zeros(self.n0(i) * self.m.nout, np.float32)
+        check(lib().nntc_b200_probe_source(self.d, i, a.ctypes.data_as(C.POINTER(C.c_float)), a.size), "probe_source")
+        return a
 
     # ---- transfers
     def set_planes(self, i, v0=None, v1=None):

@@ -47,17 +47,19 @@ def test_layout_against_reference(w, h):
         assert ps[i] == weights[i]
 
 
-def test_chain_against_reference():
+@pytest.mark.parametrize("w,h,textures,mip_min", [(52, 36, 2, 8), (33, 21, 4, 1), (40, 9, 6, 1), (61, 37, 2, 1)])
+def test_chain_against_reference(w, h, textures, mip_min):
     if not os.path.exists(O.REF_SO):
         pytest.skip("reference CPU arm not built")
     L = O.RefSession.lib()
     L.ref_source_chain.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.POINTER(C.POINTER(C.c_float))]
-    mat = M.small(9, 52, 36, textures=2)
-    outs = [np.zeros((p[1], p[0], 6), np.float32) for p in mat.planes[1:]]
+    mat = M.small(9, w, h, textures=textures, mip_min=mip_min)
+    nc = 3 * textures
+    outs = [np.zeros((p[1], p[0], nc), np.float32) for p in mat.planes[1:]]
     arr = (C.POINTER(C.c_float) * len(outs))(*[O.fptr(o) for o in outs])
     base = np.ascontiguousarray(mat.chain[0])
-    L.ref_source_chain(O.fptr(base), base.shape[1], base.shape[0], 6, len(outs), arr)
+    L.ref_source_chain(O.fptr(base), base.shape[1], base.shape[0], nc, len(outs), arr)
     for a, b in zip(outs, mat.chain[1:]):
         assert np.array_equal(a, b)
 
