@@ -79,6 +79,7 @@ int snapshot(nntc_b200_device* d, DeviceCopy& keep, bool save)
 namespace nb
 {
 int channel_copies(nntc_b200_device* d, std::vector<unsigned char>& same);
+int psnr_base(nntc_b200_device* d, const nntc_b200_model* m, double* psnr);
 }
 
 using namespace nb;
@@ -416,28 +417,9 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     cudaEventDestroy(t1);
     r->objective_passes = nntc_b200_objective_passes() - passes0;
 
-    // The per-texture 8-bit PSNR of the base level against the source bytes (src/main.cpp:2743, 3000-3060).
-    {
-        const DevPlane& p = d->planes[0];
-        const size_t n = (size_t)p.w0 * p.h0;
-        std::vector<uint8_t> rgb(n * m->nout);
-        std::vector<float> src(n * m->nout);
-        NB_TRY(nntc_b200_decode_plane(d, m, 0, rgb.data(), rgb.size()));
-        NB_TRY(download(d, src.data(), p.src, src.size() * sizeof(float)));
-        for (int t = 0; t < m->textures && t < 6; t++)
-        {
-            double se = 0.0;
-            for (size_t i = 0; i < n; i++)
-                for (int c = 0; c < 3; c++)
-                {
-                    const double want = std::lround((double)src[i * m->nout + 3 * t + c] * 255.0);
-                    const double e2 = (double)rgb[i * m->nout + 3 * t + c] - want;
-                    se += e2 * e2;
-                }
-            const double mse = se / (double)(n * 3);
-            r->psnr[t] = mse > 0.0 ? 10.0 * std::log10(255.0 * 255.0 / mse) : 99.0;
-        }
-    }
+    // The per-texture 8-bit PSNR of the base level against the source bytes (src/main.cpp:2743, 3000-3060), summed
+    // on the device.
+    NB_TRY(psnr_base(d, m, r->psnr));
     for (int i = 0; i < np; i++)
     {
         if (k0_out && k0_out[i])

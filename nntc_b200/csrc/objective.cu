@@ -10,6 +10,7 @@
 // order. The dot products use DFMA: the per-site value differs from the reference's separately-rounded multiply-add
 // in the last bits only, and E is a measurement held to 1e-9 relative of the host twin (src/objective.cu:317-380).
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -367,6 +368,58 @@ __global__ void k_decode(const float* v0, const float* v1, int w0, int h0, int w
         acc = acc < 0.0f ? 0.0f : (acc > 1.0f ? 1.0f : acc);
         out[idx * nout + r] = (uint8_t)lroundf(acc * 255.0f);
     }
+}
+
+// The per-texture squared error of the 8-bit decode against the source bytes round(255 src) (src/main.cpp:3000-3060),
+// as exact integer sums: one 64-bit total per texture, added with integer atomics, so the order does not matter.
+__global__ void k_psnr_sums(const uint8_t* rgb, const float* src, size_t n, int nout, unsigned long long* se)
+{
+    unsigned long long acc[6] = { 0, 0, 0, 0, 0, 0 };
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    {
+#pragma unroll
+        for (int t = 0; t < 6; t++)
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+            {
+                const int k = 3 * t + c;
+                if (k >= nout)
+                    continue;
+                const long long want = llround((double)src[i * nout + k] * 255.0);
+                const long long e = (long long)rgb[i * nout + k] - want;
+                acc[t] += (unsigned long long)(e * e);
+            }
+    }
+#pragma unroll
+    for (int t = 0; t < 6; t++)
+    {
+        unsigned long long v = acc[t];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v)
+            atomicAdd(se + t, v);
+    }
+}
+
+int psnr_base(nntc_b200_device* d, const nntc_b200_model* m, double* psnr)
+{
+    const DevPlane& p = d->planes[0];
+    const size_t n = (size_t)p.w0 * p.h0;
+    k_decode<<<grid_for(n, 256), 256, 0, d->stream>>>(p.v0, p.v1, p.w0, p.h0, p.w1, p.h1, d->c0, d->c1, d->nin,
+                                                      d->nout, d->weights, d->bias, d->rgb8);
+    NB_LAUNCHED();
+    unsigned long long* se = (unsigned long long*)d->radix;
+    NB_CUDA(cudaMemsetAsync(se, 0, 6 * sizeof(unsigned long long), d->stream));
+    k_psnr_sums<<<std::min(grid_for(n, 256), 148 * 8), 256, 0, d->stream>>>(d->rgb8, p.src, n, d->nout, se);
+    NB_LAUNCHED();
+    unsigned long long h[6];
+    NB_TRY(download(d, h, se, sizeof(h)));
+    for (int t = 0; t < m->textures && t < 6; t++)
+    {
+        const double mse = (double)h[t] / (double)(n * 3);
+        psnr[t] = mse > 0.0 ? 10.0 * std::log10(255.0 * 255.0 / mse) : 99.0;
+    }
+    return NNTC_B200_OK;
 }
 
 // The reported numbers from the three raw sums per plane (src/objective.cu:224-250).
