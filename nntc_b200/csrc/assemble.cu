@@ -408,9 +408,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
     // same floats) and its monomials in a fixed layout: the constant, the four linear terms, then the ten products
     // (i <= k) row by row; a narrower latent uses the entries whose indices are all below its channel count, which is
     // the reference's order
-    auto visit = [&](int px, int py, int j, float w_self, float w_other) {
-        const size_t site = (size_t)(py * V.w0 + px) * per + j;
-        const float4 y4 = __ldg(ys + site);
+    auto visit_y = [&](size_t site, float4 y4, float w_self, float w_other) {
         const float y[MAX_CH] = { y4.x, y4.y, y4.z, y4.w };
         if (slot == 0)
         {
@@ -434,6 +432,10 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
                 sums[5 + p] += scale * ((double)y[i] * (double)y[k2]);
         }
     };
+    auto visit = [&](int px, int py, int j, float w_self, float w_other) {
+        const size_t site = (size_t)(py * V.w0 + px) * per + j;
+        visit_y(site, __ldg(ys + site), w_self, w_other);
+    };
 
     const bool interior = ((A.tabled >> pl) & 1u) && tx >= GATHER_MARGIN && tx < tw_ - GATHER_MARGIN &&
                           ty >= GATHER_MARGIN && ty < th_ - GATHER_MARGIN;
@@ -441,12 +443,33 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
     {
         const int cls = LEVEL0 ? (tx & 1) + 2 * (ty & 1) : 0;
         const int bx = LEVEL0 ? tx : 4 * tx, by = LEVEL0 ? ty : 4 * ty;
-        const int e1 = A.gt.off[cls][slot + 1];
-        for (int e = A.gt.off[cls][slot]; e < e1; e++)
+        const int e0 = A.gt.off[cls][slot], e1 = A.gt.off[cls][slot + 1];
+        // one visit ahead: the next entry and its sample are loaded while this one is added (the sums still take the
+        // visits in table order)
+        auto site_of = [&](const int4& en) {
+            return (size_t)((by + ((en.x >> 8) & 0xff) - 64) * V.w0 + (bx + (en.x & 0xff) - 64)) * per + (en.x >> 16);
+        };
+        if (e0 < e1)
         {
-            const int4 en = __ldg(A.tab + e);
-            visit(bx + (en.x & 0xff) - 64, by + ((en.x >> 8) & 0xff) - 64, en.x >> 16, __int_as_float(en.y),
-                  __int_as_float(en.z));
+            int4 en = __ldg(A.tab + e0);
+            size_t site = site_of(en);
+            float4 y4 = __ldg(ys + site);
+            for (int e = e0; e < e1; e++)
+            {
+                int4 nen = en;
+                size_t nsite = site;
+                float4 ny4 = y4;
+                if (e + 1 < e1)
+                {
+                    nen = __ldg(A.tab + e + 1);
+                    nsite = site_of(nen);
+                    ny4 = __ldg(ys + nsite);
+                }
+                visit_y(site, y4, __int_as_float(en.y), __int_as_float(en.z));
+                en = nen;
+                site = nsite;
+                y4 = ny4;
+            }
         }
     }
     else
