@@ -273,14 +273,9 @@ __global__ void __launch_bounds__(OBJ_THREADS) k_objective_p(Planes P, ObjDecode
                 w01 = (1.0 - fx) * fy;
                 w11 = fx * fy;
             }
-            double sc[16];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    sc[i * 4 + q] = s[i] * c[q];
             // every row's dot product advanced together, feature by feature (each row's own sum keeps phi's order),
-            // so that NOUT independent chains of DFMAs are in flight at once
+            // so that NOUT independent chains of DFMAs are in flight at once; a product feature s_i c_q is formed
+            // once, when its turn comes, instead of being held for the whole site
             double acc[NOUT];
 #pragma unroll
             for (int r = 0; r < NOUT; r++)
@@ -297,15 +292,22 @@ __global__ void __launch_bounds__(OBJ_THREADS) k_objective_p(Planes P, ObjDecode
                     acc[r] = fma(W.w[r * 24 + 4 + h], s[h], acc[r]);
 #pragma unroll
             for (int h = 0; h < 16; h++)
+            {
+                const double sc = s[h / 4] * c[h % 4];
 #pragma unroll
                 for (int r = 0; r < NOUT; r++)
-                    acc[r] = fma(W.w[r * 24 + 8 + h], sc[h], acc[r]);
+                    acc[r] = fma(W.w[r * 24 + 8 + h], sc, acc[r]);
+            }
 #pragma unroll
             for (int r = 0; r < NOUT; r++)
             {
+                // the target's bilinear sample as a chain of fused multiply-adds (a measurement: its last bits move,
+                // within the objective's 1e-12)
                 const double t = j == 0 ? (double)__ldg(V.src + ta + r)
-                                        : w00 * (double)__ldg(V.src + ta + r) + w10 * (double)__ldg(V.src + tb + r) +
-                                              w01 * (double)__ldg(V.src + te + r) + w11 * (double)__ldg(V.src + tf + r);
+                                        : fma(w11, (double)__ldg(V.src + tf + r),
+                                              fma(w01, (double)__ldg(V.src + te + r),
+                                                  fma(w10, (double)__ldg(V.src + tb + r),
+                                                      w00 * (double)__ldg(V.src + ta + r))));
                 const double e = acc[r] - t;
                 weighted = fma(W.cw[r] * e, e, weighted);
                 if (j == 0)
