@@ -328,6 +328,10 @@ int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double
                               float* precond, double* cg_x, float* prev);
 int nntc_b200_probe_monomials(nntc_b200_device* d, int level0, double* out, size_t n);
 int nntc_b200_probe_source(nntc_b200_device* d, int plane, float* out, size_t n);   /* plane's source, HWC */
+/* y = H x for block (b)'s Gauss-Newton operator on one plane, applied matrix-free from the decode and its adjoint (the
+ * product the assembled stencil of src/solve_level1.cu:259-438 gives, to rounding). x and y: w1 h1 c1 doubles. Uses the
+ * plane's CG vectors as scratch. */
+int nntc_b200_probe_jtj_level1(nntc_b200_device* d, int k, int plane, const double* x, double* y, size_t n);
 
 #ifdef __cplusplus
 }
