@@ -59,3 +59,40 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(nntc_b200, "LIBRARY", str(tmp_path / "absent.so"))
     with pytest.raises(nntc_b200.NntcError):
         nntc_b200.lib()
+
+
+@pytest.mark.parametrize("field,value,what", [("c0", 5, "channel"), ("textures", 7, "textures"), ("nin", 3, "nin"),
+                                               ("nplanes", 0, "planes"), ("bits1", 9, "bits1")])
+def test_device_create_rejects_a_bad_model_before_any_device_work(field, value, what):
+    """Validation runs on the host first: a model the encoder cannot take is refused with a message, no GPU needed."""
+    import ctypes as C
+
+    import numpy as np
+
+    from nntc_b200 import abi, lib, materials
+
+    mat = materials.small(1, 24, 16, textures=1)
+    m = abi.make_model(mat)
+    setattr(m, field, value)
+    chain = [np.ascontiguousarray(c, np.float32) for c in mat.chain]
+    h = C.c_void_p()
+    assert lib().nntc_b200_device_create(C.byref(m), abi.float_ptrs(chain), C.byref(h)) == 1
+    assert not h.value
+    assert lib().nntc_b200_last_error().decode()
+
+
+def test_device_create_from_base_rejects_a_chain_that_is_not_the_box_halving():
+    import ctypes as C
+
+    import numpy as np
+
+    from nntc_b200 import abi, lib, materials
+
+    mat = materials.small(2, 32, 32, textures=1)
+    m = abi.make_model(mat)
+    m.w0[1] += 1
+    base = np.ascontiguousarray(mat.chain[0], np.float32).ravel()
+    h = C.c_void_p()
+    assert lib().nntc_b200_device_create_from_base(C.byref(m), base.ctypes.data_as(C.POINTER(C.c_float)),
+                                                   C.byref(h)) == 1
+    assert "halving" in lib().nntc_b200_last_error().decode()
