@@ -4,14 +4,11 @@
 // and rhs_c = sum omega v t_c; W and b follow by Gauss-Jordan with the ridge ladder {1e-9, 1e-12, 0} mean(diag A)
 // and the acceptance test on the objective's own quadratic Q (src/solve_decoder.cu:184-458), on the host.
 //
-// The accumulation, B200 shape. Every product is a float times a float, which is EXACT in double, so what matters
-// for throughput is how many shared-memory operands feed each DFMA. The reference walks the 775 entries one dot
-// product per thread (two shared loads per multiply-add). Here a block stages 256 sites' [v | t] in shared memory and
-// each thread owns a 4x4 TILE of X^T X (X = [v | t]) over a k-slice of the staged sites: 8 loads feed 16 DFMAs. Only
-// the tiles the system needs are computed: the upper triangle of V^T V and all of T^T V. Every plane of the chain is
-// in the one launch (grid.y is the plane). Each block keeps its tiles in registers over all of its chunks, folds its
-// k-slices in a fixed order and writes one partial per entry; a second kernel adds, per entry, the planes in index
-// order with their site weight omega and the blocks in index order (src/solve_decoder.cu:165-180): deterministic.
+// The accumulation, B200 shape: every product is a float times a float, exact in double, and the entries needed are
+// blocks of the Gram of Z = [phi | 1 | t] over all sites, so they run on the FP64 tensor cores (k_ls_accumulate_mma
+// below). Every plane of the chain is in the one launch (grid.y is the plane); each block writes one partial per
+// entry, and a second kernel adds, per entry, the planes in index order with their site weight omega and the blocks
+// in index order (src/solve_decoder.cu:165-180): deterministic.
 
 #include <algorithm>
 #include <cfloat>
@@ -24,51 +21,11 @@
 namespace nb
 {
 
-constexpr int LS_THREADS = 256;
 constexpr int LS_GRID = 148 * 2;   // blocks per plane
-constexpr int TILE = 4;
-constexpr int LS_STRIDE = LS_THREADS + 1;
-constexpr int VP_MAX = (MAX_NIN + 1 + TILE - 1) / TILE * TILE;   // 28
-constexpr int TP_MAX = (MAX_NOUT + TILE - 1) / TILE * TILE;      // 20
 
 __host__ __device__ inline int tri_index(int i, int j, int mm)
 {
     return i * mm - i * (i - 1) / 2 + (j - i);
-}
-
-// The tiles a launch computes: (row tile, col tile) with row tiles 0..nv-1 over V (upper triangle, col >= row) and
-// nv..nv+nt-1 over T (every col tile of V).
-struct LsShape
-{
-    int mm, nout, nv, nt, tiles, ks;
-    int trow[64], tcol[64];
-};
-
-inline LsShape ls_shape(int nin, int nout)
-{
-    LsShape s{};
-    s.mm = nin + 1;
-    s.nout = nout;
-    s.nv = (s.mm + TILE - 1) / TILE;
-    s.nt = (nout + TILE - 1) / TILE;
-    int n = 0;
-    for (int i = 0; i < s.nv; i++)
-        for (int j = i; j < s.nv; j++)
-        {
-            s.trow[n] = i;
-            s.tcol[n] = j;
-            n++;
-        }
-    for (int i = 0; i < s.nt; i++)
-        for (int j = 0; j < s.nv; j++)
-        {
-            s.trow[n] = s.nv + i;
-            s.tcol[n] = j;
-            n++;
-        }
-    s.tiles = n;
-    s.ks = LS_THREADS / n;   // k-slices of the staged chunk
-    return s;
 }
 
 struct LsArgs
@@ -76,156 +33,6 @@ struct LsArgs
     double* partial;   // [plane][entry][LS_GRID]
     int entries;
 };
-
-__global__ void __launch_bounds__(LS_THREADS) k_ls_accumulate(Planes P, LsShape S, LsArgs A)
-{
-    extern __shared__ double ls_sh[];
-    double* fold = ls_sh;                              // LS_THREADS doubles
-    float* sx = (float*)(ls_sh + LS_THREADS);          // [col][site]: V columns 0..VP-1, then T columns
-    const int pl = blockIdx.y;
-    const PlaneView& V = P.p[pl];
-    const int c0 = P.c0, c1 = P.c1, nin = P.nin, nout = P.nout, kc = P.kc, mm = S.mm;
-    const int VP = S.nv * TILE, TP = S.nt * TILE;
-    const int per_pixel = 1 + kc;
-    const size_t sites = (size_t)V.w0 * V.h0 * per_pixel;
-    const size_t chunks = (sites + LS_THREADS - 1) / LS_THREADS;
-    const int tid = threadIdx.x;
-    const int tile = tid % S.tiles, kg = tid / S.tiles;
-    const bool worker = kg < S.ks;
-    const int r0 = S.trow[tile] * TILE, cc0 = S.tcol[tile] * TILE;   // row in [V|T] column space, col in V
-    double acc[TILE][TILE];
-#pragma unroll
-    for (int a = 0; a < TILE; a++)
-#pragma unroll
-        for (int b = 0; b < TILE; b++)
-            acc[a][b] = 0.0;
-
-    for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
-    {
-        const size_t si = chunk * LS_THREADS + tid;
-        __syncthreads();   // the previous chunk's tiles have finished reading
-        // The site's row [phi | 1 | t] staged straight into shared memory, each value with the solver's arithmetic
-        // (src/sample.cuh:154-178); a site outside the plane stages a row of zeros.
-        if (si < sites)
-        {
-            const size_t pixel = si / (size_t)per_pixel;
-            const int j = (int)(si % (size_t)per_pixel);
-            const int px = (int)(pixel % (size_t)V.w0), py = (int)(pixel / (size_t)V.w0);
-            float dx, dy;
-            site_offset(kc, j, px, py, dx, dy);
-            float s[MAX_CH], c[MAX_CH];
-            const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
-            blend_u<MAX_CH>(V.v1, V.w1, c1, t1, c);
-            Tap t0{};
-            float w4[4];
-            if (j == 0)
-            {
-#pragma unroll
-                for (int i = 0; i < MAX_CH; i++)
-                    if (i < c0)
-                        s[i] = __ldg(V.v0 + pixel * c0 + i);
-            }
-            else
-            {
-                t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
-                blend_u<MAX_CH>(V.v0, V.w0, c0, t0, s);
-                tap_weights(t0, w4);
-            }
-            int q = 0;
-#pragma unroll
-            for (int jj = 0; jj < MAX_CH; jj++)
-                if (jj < c1)
-                    sx[(q++) * LS_STRIDE + tid] = c[jj];
-#pragma unroll
-            for (int i = 0; i < MAX_CH; i++)
-                if (i < c0)
-                    sx[(q++) * LS_STRIDE + tid] = s[i];
-#pragma unroll
-            for (int i = 0; i < MAX_CH; i++)
-#pragma unroll
-                for (int jj = 0; jj < MAX_CH; jj++)
-                    if (i < c0 && jj < c1)
-                        sx[(q++) * LS_STRIDE + tid] = s[i] * c[jj];
-            sx[nin * LS_STRIDE + tid] = 1.0f;
-            for (int r = 0; r < nout; r++)
-            {
-                float t;
-                if (j == 0)
-                    t = __ldg(V.src + pixel * nout + r);
-                else
-                    t = w4[0] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x0) * nout + r) +
-                        w4[1] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x1) * nout + r) +
-                        w4[2] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x0) * nout + r) +
-                        w4[3] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x1) * nout + r);
-                sx[(VP + r) * LS_STRIDE + tid] = t;
-            }
-        }
-        else
-        {
-            for (int i = 0; i < mm; i++)
-                sx[i * LS_STRIDE + tid] = 0.0f;
-            for (int r = 0; r < nout; r++)
-                sx[(VP + r) * LS_STRIDE + tid] = 0.0f;
-        }
-        for (int i = mm; i < VP; i++)
-            sx[i * LS_STRIDE + tid] = 0.0f;
-        for (int r = nout; r < TP; r++)
-            sx[(VP + r) * LS_STRIDE + tid] = 0.0f;
-        __syncthreads();
-        if (worker)
-        {
-            const float* rowp = sx + r0 * LS_STRIDE;
-            const float* colp = sx + cc0 * LS_STRIDE;
-            for (int p = kg; p < LS_THREADS; p += S.ks)
-            {
-                double a[TILE], b[TILE];
-#pragma unroll
-                for (int q = 0; q < TILE; q++)
-                {
-                    a[q] = (double)rowp[q * LS_STRIDE + p];
-                    b[q] = (double)colp[q * LS_STRIDE + p];
-                }
-#pragma unroll
-                for (int x = 0; x < TILE; x++)
-#pragma unroll
-                    for (int y = 0; y < TILE; y++)
-                        acc[x][y] = fma(a[x], b[y], acc[x][y]);
-            }
-        }
-    }
-
-    // Fold the k-slices in order 0..ks-1, entry by entry, and write the entries this tile owns.
-#pragma unroll
-    for (int x = 0; x < TILE; x++)
-#pragma unroll
-        for (int y = 0; y < TILE; y++)
-        {
-            __syncthreads();
-            fold[tid] = acc[x][y];
-            __syncthreads();
-            if (worker && kg == 0)
-            {
-                double s = 0.0;
-                for (int g = 0; g < S.ks; g++)
-                    s += fold[g * S.tiles + tile];
-                const int row = r0 + x, col = cc0 + y;
-                int e = -1;
-                if (row < VP)
-                {
-                    if (row < mm && col < mm && col >= row)
-                        e = tri_index(row, col, mm);
-                }
-                else
-                {
-                    const int c = row - VP;
-                    if (c < nout && col < mm)
-                        e = S.mm * (S.mm + 1) / 2 + c * mm + col;
-                }
-                if (e >= 0)
-                    A.partial[((size_t)pl * A.entries + e) * LS_GRID + blockIdx.x] = s;
-            }
-        }
-}
 
 // ---- the accumulation on the FP64 tensor cores
 //
@@ -409,8 +216,7 @@ __global__ void k_ls_reduce(const double* partial, int entries, int planes, cons
 
 int normal_equations(nntc_b200_device* d, int k, const double* per_site, double* ms)
 {
-    const LsShape S = ls_shape(d->nin, d->nout);
-    const int mm = S.mm;
+    const int mm = d->nin + 1;
     const int entries = mm * (mm + 1) / 2 + d->nout * mm;
     if (!d->ls_partial)
         NB_CUDA(cudaMalloc(&d->ls_partial, ((size_t)d->planes.size() * entries * LS_GRID + MAX_PLANES) *
@@ -427,7 +233,6 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
     k_ls_accumulate_mma<<<grid, NE_THREADS, shared, d->stream>>>(P, LsArgs{ d->ls_partial, entries });
     NB_TRY(ktimer_end(d));
-    (void)S;
     NB_LAUNCHED();
     k_ls_reduce<<<grid_for((size_t)entries, 128), 128, 0, d->stream>>>(d->ls_partial, entries, P.n, omega,
                                                                       d->reduction);
