@@ -21,7 +21,7 @@
 namespace nb
 {
 
-constexpr int LS_GRID = 148 * 2;   // blocks per plane
+constexpr int LS_GRID = 148 * 4;   // blocks per plane: four per SM keep the base plane at full occupancy
 
 __host__ __device__ inline int tri_index(int i, int j, int mm)
 {
