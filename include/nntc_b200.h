@@ -332,6 +332,8 @@ int nntc_b200_probe_source(nntc_b200_device* d, int plane, float* out, size_t n)
  * product the assembled stencil of src/solve_level1.cu:259-438 gives, to rounding). x and y: w1 h1 c1 doubles. Uses the
  * plane's CG vectors as scratch. */
 int nntc_b200_probe_jtj_level1(nntc_b200_device* d, int k, int plane, const double* x, double* y, size_t n);
+/* The same for block (c')'s operator over level 0 (src/solve_level1.cu:440-581): x and y w0 h0 c0 doubles; bc8 only. */
+int nntc_b200_probe_jtj_level0(nntc_b200_device* d, int k, int plane, const double* x, double* y, size_t n);
 
 #ifdef __cplusplus
 }

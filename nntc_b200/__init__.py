@@ -86,6 +86,7 @@ PROTOTYPES = {
     "nntc_b200_probe_monomials": (_I, [_P, _I, _PD, _S]),
     "nntc_b200_probe_source": (_I, [_P, _I, _PF, _S]),
     "nntc_b200_probe_jtj_level1": (_I, [_P, _I, _I, _PD, _PD, _S]),
+    "nntc_b200_probe_jtj_level0": (_I, [_P, _I, _I, _PD, _PD, _S]),
 }
 
 

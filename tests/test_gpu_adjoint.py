@@ -1,7 +1,7 @@
-"""The decode's derivatives, checked two ways on a B200 (block (b), level 1).
+"""The decode's derivatives, checked two ways on a B200 (block (b) over level 1, block (c') over level 0).
 
 - The assembled stencil against the fused forward/adjoint operator: H x from the stencil the assembly stored (the
-  reference's per-texel blocks, src/solve_level1.cu:259-438) and from nntc_b200_probe_jtj_level1, which applies
+  reference's per-texel blocks, src/solve_level1.cu:259-581) and from nntc_b200_probe_jtj_level{1,0}, which apply
   J^T diag(cw) J site by site without assembling anything, agree to 1e-12 relative on random vectors.
 - The assembled gradient against central finite differences of the objective: for a random direction d the change of
   a plane's E between v + h d and v - h d is 4 g.d / (sum cw x sites) (E is quadratic in level 1), to 1e-6 relative
@@ -47,31 +47,35 @@ def stencil_product(stencil, x, w, h, c):
     return y.ravel()
 
 
+@pytest.mark.parametrize("level0", [False, True])
 @pytest.mark.parametrize("textures,c0,c1,w,h", [(2, 4, 4, 72, 40), (1, 2, 4, 61, 37), (2, 3, 2, 64, 64)])
-def test_matrix_free_operator_matches_the_assembled_stencil(textures, c0, c1, w, h):
+def test_matrix_free_operator_matches_the_assembled_stencil(textures, c0, c1, w, h, level0):
     mat = materials.small(80 + w, w, h, textures=textures, c0=c0, c1=c1)
     dw, db, v0, v1 = random_state(mat, w + 7 * h)
     rng = np.random.default_rng(3)
+    probe = lib().nntc_b200_probe_jtj_level0 if level0 else lib().nntc_b200_probe_jtj_level1
     with Session(mat) as s:
         for i in range(len(mat.planes)):
             s.set_planes(i, v0[i], v1[i])
         s.set_decoder(dw, db)
         s.set_grids(np.full(c0, -1.0), np.full(c0, 1.0))
-        s.block(False)   # assembles every plane's level-1 stencil
+        s.block(level0)   # assembles every plane's stencil of that latent
+        c = c0 if level0 else c1
         for i, p in enumerate(mat.planes):
-            w1, h1 = p[2], p[3]
-            ws = s.workspace(i, False)
+            uw, uh = (p[0], p[1]) if level0 else (p[2], p[3])
+            ws = s.workspace(i, level0)
             for _ in range(2):
-                x = rng.standard_normal(w1 * h1 * c1)
-                want = stencil_product(ws["stencil"], x, w1, h1, c1)
+                x = rng.standard_normal(uw * uh * c)
+                want = stencil_product(ws["stencil"], x, uw, uh, c)
                 got = np.zeros_like(x)
-                check(lib().nntc_b200_probe_jtj_level1(s.d, 4, i, x.ctypes.data_as(C.POINTER(C.c_double)),
-                                                       got.ctypes.data_as(C.POINTER(C.c_double)), got.size), "jtj")
+                check(probe(s.d, 4, i, x.ctypes.data_as(C.POINTER(C.c_double)),
+                            got.ctypes.data_as(C.POINTER(C.c_double)), got.size), "jtj")
                 assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), (i, np.abs(got - want).max())
 
 
+@pytest.mark.parametrize("level0", [False, True])
 @pytest.mark.parametrize("textures,c0,c1,w,h", [(2, 4, 4, 72, 40), (1, 2, 4, 61, 37)])
-def test_gradient_matches_central_differences(textures, c0, c1, w, h):
+def test_gradient_matches_central_differences(textures, c0, c1, w, h, level0):
     mat = materials.small(90 + w, w, h, textures=textures, c0=c0, c1=c1)
     dw, db, v0, v1 = random_state(mat, 5 * w + h)
     rng = np.random.default_rng(4)
@@ -81,20 +85,21 @@ def test_gradient_matches_central_differences(textures, c0, c1, w, h):
             s.set_planes(i, v0[i], v1[i])
         s.set_decoder(dw, db)
         s.set_grids(np.full(c0, -1.0), np.full(c0, 1.0))
-        s.block(False)   # assembles the gradient at the planes as set, then the solve moves them
+        s.block(level0)   # assembles the gradient at the planes as set, then the solve moves them
         sum_cw = float(np.sum(np.array(s.m.cw[: s.m.nout], np.float64)))
         for i, p in enumerate(mat.planes[:2]):
-            g = s.workspace(i, False)["grad"]
-            prev = v1[i]   # the point the gradient was assembled at
+            g = s.workspace(i, level0)["grad"]
+            prev = (v0 if level0 else v1)[i]   # the point the gradient was assembled at
             d = rng.standard_normal(prev.size)
             hstep = 1e-3
             vp = (prev + hstep * d).astype(np.float32)
             vm = (prev - hstep * d).astype(np.float32)
-            s.set_planes(i, v1=vp)
+            put = (lambda v: s.set_planes(i, v0=v)) if level0 else (lambda v: s.set_planes(i, v1=v))
+            put(vp)
             ep = s.objective(k).e_plane[i]
-            s.set_planes(i, v1=vm)
+            put(vm)
             em = s.objective(k).e_plane[i]
-            s.set_planes(i, v1=prev)
+            put(prev)
             delta = (vp.astype(np.float64) - vm.astype(np.float64)) / 2.0
             sites = float(p[0]) * float(p[1]) * (1 + k)
             fd = (ep - em) * sum_cw * sites / 4.0
