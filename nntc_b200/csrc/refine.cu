@@ -292,6 +292,19 @@ __device__ __forceinline__ double row_of(const double (&uv)[R], int idx)
     return v;
 }
 
+// The same for an idx every lane holds alike: the slot it sits in is then the same on every lane too, so only that
+// slot is shuffled.
+template <int R>
+__device__ __forceinline__ double row_of_uniform(const double (&uv)[R], int idx)
+{
+    double x = uv[0];
+#pragma unroll
+    for (int q = 1; q < R; q++)
+        if ((idx >> 5) == q)
+            x = uv[q];
+    return __shfl_sync(0xffffffffu, x, idx & 31);
+}
+
 // The sixteen lanes' terms folded serially in texel order, the same on every lane.
 __device__ __forceinline__ double fold16(double v)
 {
@@ -552,27 +565,23 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
             for (int t = 0; t < 16; t++)
             {
                 const int i = t * C0 + c;
-                const double b = a1[i] + row_of(uv, i);
+                const double b = a1[i] + row_of_uniform(uv, i);
                 const double a = S[t * TS + c * C0 + c];
                 const int cur = s_sel[c * 16 + t];
                 const double now = __shfl_sync(0xffffffffu, cand, cur);
                 const double d = cand - now;
                 const double de = 2.0 * b * d + a * d * d;
-                double v = de < 0.0 ? de : 0.0, mv = d;
-                int id = de < 0.0 ? k8 : 8;
+                // the lowest change of the group's eight candidates (a candidate that does not lower E counts as 0),
+                // then the first candidate that reaches it: the one the reference's in-order scan with a strict `<`
+                // keeps
+                const double mine = de < 0.0 ? de : 0.0;
+                double v = mine;
 #pragma unroll
                 for (int o = 1; o < 8; o <<= 1)
-                {
-                    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-                    const double om = __shfl_xor_sync(0xffffffffu, mv, o);
-                    const int oi = __shfl_xor_sync(0xffffffffu, id, o);
-                    if (ov < v || (ov == v && oi < id))
-                    {
-                        v = ov;
-                        mv = om;
-                        id = oi;
-                    }
-                }
+                    v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+                const unsigned hits = __ballot_sync(0xffffffffu, lane < 8 && mine == v);
+                const int id = __ffs(hits) - 1;
+                const double mv = __shfl_sync(0xffffffffu, d, id & 7);
                 // v, mv and id are the same on every lane
                 if (v < 0.0)
                 {
