@@ -578,7 +578,8 @@ static int device_create_impl(const nntc_b200_model* m, const float* const* chai
         size_t blocks = 0;
         for (const DevPlane& p : d->planes)
             blocks += ((size_t)p.w0 * p.h0 + THREADS - 1) / THREADS;
-        NB_ALLOC(d->obj_partial, (blocks * 3 + 3 * MAX_PLANES) * sizeof(double));
+        // (the objective's 128-thread blocks: two partials per 256-pixel block)
+        NB_ALLOC(d->obj_partial, (2 * blocks * 3 + 3 * MAX_PLANES) * sizeof(double));
     }
     d->scratch_floats = std::max(max0 * (size_t)m->c0, max1 * (size_t)m->c1);
     d->scratch_bytes = d->scratch_floats;

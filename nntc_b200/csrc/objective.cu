@@ -22,6 +22,7 @@ namespace nb
 {
 
 constexpr int OBJ_THREADS = 256;
+constexpr int OBJ_P_THREADS = 128;   // k_objective_p's blocks: smaller blocks fit five per SM at its register count
 
 struct ObjArgs
 {
@@ -220,7 +221,7 @@ struct ObjDecoder
 // k_objective for a material of NOUT outputs (3 per texture), the decoder in the launch's parameters. The same sites,
 // the same operations in the same order, so the same bits as k_objective.
 template <int NOUT>
-__global__ void __launch_bounds__(OBJ_THREADS) k_objective_p(Planes P, ObjDecoder W, double* partial)
+__global__ void __launch_bounds__(OBJ_P_THREADS, 5) k_objective_p(Planes P, ObjDecoder W, double* partial)
 {
     __shared__ double red[32];
     const int c0 = P.c0, c1 = P.c1, kc = P.kc;
@@ -330,11 +331,11 @@ __global__ void __launch_bounds__(OBJ_THREADS) k_objective_p(Planes P, ObjDecode
 }
 
 // One block per plane: the plane's block partials added in a fixed order (a strided pass, then a fixed tree).
-__global__ void k_objective_reduce(Planes P, const double* partial, int nblocks, double* out)
+__global__ void k_objective_reduce(Planes P, const double* partial, int nblocks, double* out, int bthreads)
 {
     __shared__ double red[32];
     const int pl = blockIdx.x;
-    const long long b0 = P.start[pl] / OBJ_THREADS, b1 = P.start[pl + 1] / OBJ_THREADS;
+    const long long b0 = P.start[pl] / bthreads, b1 = P.start[pl + 1] / bthreads;
     for (int row = 0; row < 3; row++)
     {
         double s = 0.0;
@@ -455,7 +456,8 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
 {
     Planes P = planes_for(d, 0, [&](int i) { return (size_t)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0; });
     P.kc = k;
-    const int nblocks = (int)(P.start[P.n] / OBJ_THREADS);
+    const int bthreads = d->nout % 3 == 0 && d->nout <= 18 ? OBJ_P_THREADS : OBJ_THREADS;
+    const int nblocks = (int)(P.start[P.n] / bthreads);
     // device_create sized obj_partial for this layout: 3 doubles per pixel block, then 3 sums per plane.
     double* sums = d->obj_partial + (size_t)nblocks * 3;
     // the decoder as the device holds it, in the 24-slot row layout (a channel the layout does not use has weight 0)
@@ -484,18 +486,18 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
     NB_TRY(ktimer_begin(d, NNTC_B200_K_OBJECTIVE));
     switch (nout)
     {
-    case 3: k_objective_p<3><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 6: k_objective_p<6><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 9: k_objective_p<9><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 12: k_objective_p<12><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 15: k_objective_p<15><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 18: k_objective_p<18><<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 3: k_objective_p<3><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 6: k_objective_p<6><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 9: k_objective_p<9><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 12: k_objective_p<12><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 15: k_objective_p<15><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 18: k_objective_p<18><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
     default:
         k_objective<<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, ObjArgs{ d->weights, d->bias, d->cw, d->obj_partial });
     }
     NB_TRY(ktimer_end(d));
     NB_LAUNCHED();
-    k_objective_reduce<<<P.n, 256, 0, d->stream>>>(P, d->obj_partial, nblocks, sums);
+    k_objective_reduce<<<P.n, 256, 0, d->stream>>>(P, d->obj_partial, nblocks, sums, bthreads);
     NB_LAUNCHED();
     NB_TRY(block_end(d, ms));
     acc.assign((size_t)3 * P.n, 0.0);
@@ -744,7 +746,7 @@ extern "C" int nntc_b200_objective_plane_noalloc(const float* v0, int w0, int h0
     const cudaStream_t s = (cudaStream_t)stream;
     k_objective<<<nblocks, OBJ_THREADS, 0, s>>>(P, ObjArgs{ weights, bias, cw, partial });
     NB_LAUNCHED();
-    k_objective_reduce<<<1, 256, 0, s>>>(P, partial, nblocks, sums);
+    k_objective_reduce<<<1, 256, 0, s>>>(P, partial, nblocks, sums, OBJ_THREADS);
     NB_LAUNCHED();
     return NNTC_B200_OK;
 }
