@@ -21,7 +21,6 @@
 namespace nb
 {
 
-constexpr int LS_GRID = 148 * 4;   // blocks per plane: four per SM keep the base plane at full occupancy
 
 __host__ __device__ inline int tri_index(int i, int j, int mm)
 {
@@ -218,9 +217,6 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
 {
     const int mm = d->nin + 1;
     const int entries = mm * (mm + 1) / 2 + d->nout * mm;
-    if (!d->ls_partial)
-        NB_CUDA(cudaMalloc(&d->ls_partial, ((size_t)d->planes.size() * entries * LS_GRID + MAX_PLANES) *
-                                               sizeof(double)));
     double* omega = d->ls_partial + (size_t)d->planes.size() * entries * LS_GRID;
     NB_CUDA(cudaMemcpyAsync(omega, per_site, d->planes.size() * sizeof(double), cudaMemcpyHostToDevice, d->stream));
     Planes P = planes_for(d, 0, [&](int) { return (size_t)0; });

@@ -282,28 +282,127 @@ using namespace nb;
 namespace
 {
 
-template <typename T>
-int dev_alloc(nntc_b200_device* d, T** p, size_t bytes)
+// Every buffer of the device model is a 256-byte-aligned slice of one device allocation, the arena: a create costs
+// one cudaMalloc and a destroy one cudaFree, and nothing is allocated while an encode runs. The layout below runs
+// twice, once to measure (no base) and once to carve.
+struct Carver
 {
-    *p = nullptr;
-    if (bytes == 0)
-        return NNTC_B200_OK;
-    const cudaError_t err = cudaMalloc(p, bytes);
+    char* base = nullptr;
+    size_t at = 0;
+    template <typename T>
+    void operator()(T*& p, size_t bytes)
+    {
+        at = (at + 255) / 256 * 256;
+        p = base && bytes ? reinterpret_cast<T*>(base + at) : nullptr;
+        at += bytes;
+    }
+};
+
+void layout(nntc_b200_device* d, const nntc_b200_model* m, Carver& take)
+{
+    size_t max0 = 0, max1 = 0, blocks = 0, sites = 0;
+    for (DevPlane& p : d->planes)
+    {
+        const size_t n0 = (size_t)p.w0 * p.h0, n1 = (size_t)p.w1 * p.h1;
+        max0 = std::max(max0, n0);
+        max1 = std::max(max1, n1);
+        blocks += (n0 + THREADS - 1) / THREADS;
+        sites += n0 * 5;
+        take(p.src, n0 * m->nout * sizeof(float));
+        take(p.v0, n0 * m->c0 * sizeof(float));
+        take(p.v1, n1 * m->c1 * sizeof(float));
+        take(p.k0, n0 * m->c0);
+        take(p.k1, n1 * m->c1);
+        for (int lv = 0; lv < (m->l0_bc8 ? 2 : 1); lv++)
+        {
+            Work& w = p.work[lv];
+            const size_t t = w.texels(), c = (size_t)w.c;
+            take(w.stencil, t * SLOTS * c * c * sizeof(double));
+            take(w.grad, t * c * sizeof(double));
+            take(w.precond, t * c * c * sizeof(float));
+            take(w.x, t * c * sizeof(double));
+            take(w.r, t * c * sizeof(double));
+            take(w.z, t * c * sizeof(double));
+            take(w.p, t * c * sizeof(double));
+            take(w.ap, t * c * sizeof(double));
+            take(w.prev, t * c * sizeof(float));
+        }
+        if (m->l0_bc8)
+        {
+            take(p.bc_ep, p.blocks() * m->c0 * 2);
+            take(p.bc_sel, p.blocks() * m->c0 * 16);
+        }
+    }
+    take(d->weights, (size_t)m->nout * m->nin * sizeof(float));
+    take(d->bias, (size_t)m->nout * sizeof(float));
+    take(d->palette, (size_t)MAX_CH * 16 * sizeof(float));
+    take(d->lo1, MAX_CH * sizeof(float));
+    take(d->hi1, MAX_CH * sizeof(float));
+    if (m->l0_bc8)
+    {
+        take(d->lo0, MAX_CH * sizeof(float));
+        take(d->hi0, MAX_CH * sizeof(float));
+        take(d->mono[1], (size_t)monomial_count(m->c1) * m->c0 * m->c0 * sizeof(double));
+    }
+    take(d->mono[0], (size_t)monomial_count(m->c0) * m->c1 * m->c1 * sizeof(double));
+    take(d->cw, (size_t)m->nout * sizeof(float));
+    // one partial per 256-item block of every plane's padded range and per reduction row (level 0 is the wider
+    // unknown, so its texels bound every launch's block count)
+    take(d->partial, (size_t)RROWS * blocks * sizeof(double));
+    take(d->scalars, (size_t)MAX_PLANES * S_COUNT * sizeof(double));
+    take(d->counters, (size_t)COUNTERS * sizeof(unsigned int));
+    const int mm = m->nin + 1;
+    const size_t entries = (size_t)(mm * (mm + 1) / 2 + m->nout * mm);
+    take(d->reduction, entries * sizeof(double));
+    // the normal equations' per-block partials of every plane, then one per-site weight per plane
+    take(d->ls_partial, (d->planes.size() * entries * LS_GRID + MAX_PLANES) * sizeof(double));
+    take(d->bc_stats, (size_t)MAX_PLANES * 2 * sizeof(double));
+    take(d->radix, (size_t)std::max(2 * MAX_CH * 2048, MAX_NOUT * MAX_NOUT) * sizeof(unsigned int));
+    // the assembly's per-site gradient terms: every site of every plane at the largest K (4), one double per channel
+    // of the wider unknown; and every site's sample of the other latent
+    d->site_terms_count = sites * (size_t)std::max(m->c0, m->c1);
+    take(d->site_terms, d->site_terms_count * sizeof(double));
+    take(d->site_y, sites * 4 * sizeof(float));
+    take(d->gtab[0], (size_t)GATHER_TABLE_MAX * 16);
+    take(d->gtab[1], (size_t)GATHER_TABLE_MAX * 16);
+    // the objective's partials: two triples per 256-pixel block (its blocks are 128 threads), then three sums per plane
+    take(d->obj_partial, (2 * blocks * 3 + 3 * MAX_PLANES) * sizeof(double));
+    d->scratch_floats = std::max(max0 * (size_t)m->c0, max1 * (size_t)m->c1);
+    d->scratch_bytes = d->scratch_floats;
+    take(d->scratch, d->scratch_floats * sizeof(float));
+    take(d->scratch8, d->scratch_bytes);
+    take(d->rgb8, max0 * m->nout);
+    take(d->means, max1 * m->nout * sizeof(float));
+    if (m->init0_residual)
+        take(d->resid, max0 * m->nout * sizeof(float));
+    take(d->cov, (size_t)(MAX_NOUT + MAX_NOUT * MAX_NOUT) * COV_GRID * sizeof(double));
+    take(d->hist, (size_t)HIST_BINS * sizeof(unsigned long long));
+    if (m->l0_bc8)
+    {
+        size_t kept = 0;
+        for_each_kept(d, [&](void*, size_t b) { kept += (b + 255) / 256 * 256; });
+        take(d->keep, kept);
+    }
+}
+
+int arena_alloc(nntc_b200_device* d, size_t bytes)
+{
+    const cudaError_t err = cudaMalloc(&d->arena, bytes);
     if (err == cudaErrorMemoryAllocation)
     {
+        d->arena = nullptr;
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         char buf[512];
         snprintf(buf, sizeof(buf),
-                 "out of GPU memory allocating %.1f MB for the encode's device model (%.1f MB already allocated, "
-                 "%zu/%zu MB free): the material is too large for this GPU; try fewer or smaller textures, or fewer "
-                 "latent channels",
-                 bytes / 1048576.0, d->bytes / 1048576.0, free_b >> 20, total_b >> 20);
+                 "out of GPU memory allocating %.1f MB for the encode's device model (%zu/%zu MB free): the material "
+                 "is too large for this GPU; try fewer or smaller textures, or fewer latent channels",
+                 bytes / 1048576.0, free_b >> 20, total_b >> 20);
         set_error(NNTC_B200_ERR_OOM, buf);
         return NNTC_B200_ERR_OOM;
     }
     NB_CUDA(err);
-    d->bytes += bytes;
+    d->bytes = bytes;
     return NNTC_B200_OK;
 }
 
@@ -453,13 +552,6 @@ static int device_create_impl(const nntc_b200_model* m, const float* const* chai
         nntc_b200_device_destroy(d);
         return st;
     };
-#define NB_ALLOC(ptr, bytes)                                                                                          \
-    do                                                                                                                \
-    {                                                                                                                 \
-        const int st_ = dev_alloc(d, &(ptr), (bytes));                                                                \
-        if (st_)                                                                                                      \
-            return fail(st_);                                                                                         \
-    } while (0)
 #define NB_CK(call)                                                                                                   \
     do                                                                                                                \
     {                                                                                                                 \
@@ -473,7 +565,6 @@ static int device_create_impl(const nntc_b200_model* m, const float* const* chai
         NB_CK(cudaEventCreate(&d->ev[e]));
 
     d->planes.resize((size_t)m->nplanes);
-    size_t max0 = 0, max1 = 0;
     for (int i = 0; i < m->nplanes; i++)
     {
         DevPlane& p = d->planes[(size_t)i];
@@ -481,14 +572,28 @@ static int device_create_impl(const nntc_b200_model* m, const float* const* chai
         p.h0 = m->h0[i];
         p.w1 = m->w1[i];
         p.h1 = m->h1[i];
+        for (int lv = 0; lv < (m->l0_bc8 ? 2 : 1); lv++)
+        {
+            Work& w = p.work[lv];
+            w.w = lv ? p.w0 : p.w1;
+            w.h = lv ? p.h0 : p.h1;
+            w.c = lv ? m->c0 : m->c1;
+        }
+    }
+    {
+        Carver measure;
+        layout(d, m, measure);
+        const int st = arena_alloc(d, measure.at);
+        if (st)
+            return fail(st);
+        Carver carve;
+        carve.base = (char*)d->arena;
+        layout(d, m, carve);
+    }
+    for (int i = 0; i < m->nplanes; i++)
+    {
+        DevPlane& p = d->planes[(size_t)i];
         const size_t n0 = (size_t)p.w0 * p.h0, n1 = (size_t)p.w1 * p.h1;
-        max0 = std::max(max0, n0);
-        max1 = std::max(max1, n1);
-        NB_ALLOC(p.src, n0 * m->nout * sizeof(float));
-        NB_ALLOC(p.v0, n0 * m->c0 * sizeof(float));
-        NB_ALLOC(p.v1, n1 * m->c1 * sizeof(float));
-        NB_ALLOC(p.k0, n0 * m->c0);
-        NB_ALLOC(p.k1, n1 * m->c1);
         if (chain[i])
             NB_CK(cudaMemcpy(p.src, chain[i], n0 * m->nout * sizeof(float), cudaMemcpyHostToDevice));
         NB_CK(cudaMemset(p.v0, 0, n0 * m->c0 * sizeof(float)));
@@ -498,103 +603,38 @@ static int device_create_impl(const nntc_b200_model* m, const float* const* chai
         for (int lv = 0; lv < (m->l0_bc8 ? 2 : 1); lv++)
         {
             Work& w = p.work[lv];
-            w.w = lv ? p.w0 : p.w1;
-            w.h = lv ? p.h0 : p.h1;
-            w.c = lv ? m->c0 : m->c1;
             const size_t t = w.texels(), c = (size_t)w.c;
-            NB_ALLOC(w.stencil, t * SLOTS * c * c * sizeof(double));
-            NB_ALLOC(w.grad, t * c * sizeof(double));
-            NB_ALLOC(w.precond, t * c * c * sizeof(float));
-            NB_ALLOC(w.x, t * c * sizeof(double));
-            NB_ALLOC(w.r, t * c * sizeof(double));
-            NB_ALLOC(w.z, t * c * sizeof(double));
-            NB_ALLOC(w.p, t * c * sizeof(double));
-            NB_ALLOC(w.ap, t * c * sizeof(double));
-            NB_ALLOC(w.prev, t * c * sizeof(float));
             NB_CK(cudaMemset(w.x, 0, t * c * sizeof(double)));
             NB_CK(cudaMemset(w.prev, 0, t * c * sizeof(float)));
         }
         if (m->l0_bc8)
         {
-            NB_ALLOC(p.bc_ep, p.blocks() * m->c0 * 2);
-            NB_ALLOC(p.bc_sel, p.blocks() * m->c0 * 16);
             NB_CK(cudaMemset(p.bc_ep, 0, p.blocks() * m->c0 * 2));
             NB_CK(cudaMemset(p.bc_sel, 0, p.blocks() * m->c0 * 16));
         }
     }
-    NB_ALLOC(d->weights, (size_t)m->nout * m->nin * sizeof(float));
-    NB_ALLOC(d->bias, (size_t)m->nout * sizeof(float));
     // The decoder starts at zero: the first objective pass measures the zero decoder (src/init.cu:262-267).
     NB_CK(cudaMemset(d->weights, 0, (size_t)m->nout * m->nin * sizeof(float)));
     NB_CK(cudaMemset(d->bias, 0, (size_t)m->nout * sizeof(float)));
-    NB_ALLOC(d->palette, (size_t)MAX_CH * 16 * sizeof(float));
-    NB_ALLOC(d->lo1, MAX_CH * sizeof(float));
-    NB_ALLOC(d->hi1, MAX_CH * sizeof(float));
     NB_CK(cudaMemset(d->palette, 0, (size_t)MAX_CH * 16 * sizeof(float)));
     NB_CK(cudaMemset(d->lo1, 0, MAX_CH * sizeof(float)));
     NB_CK(cudaMemset(d->hi1, 0, MAX_CH * sizeof(float)));
     if (m->l0_bc8)
     {
-        NB_ALLOC(d->lo0, MAX_CH * sizeof(float));
-        NB_ALLOC(d->hi0, MAX_CH * sizeof(float));
         NB_CK(cudaMemset(d->lo0, 0, MAX_CH * sizeof(float)));
         NB_CK(cudaMemset(d->hi0, 0, MAX_CH * sizeof(float)));
-        NB_ALLOC(d->mono[1], (size_t)monomial_count(m->c1) * m->c0 * m->c0 * sizeof(double));
     }
-    NB_ALLOC(d->mono[0], (size_t)monomial_count(m->c0) * m->c1 * m->c1 * sizeof(double));
-    NB_ALLOC(d->cw, (size_t)m->nout * sizeof(float));
     NB_CK(cudaMemcpy(d->cw, m->cw, (size_t)m->nout * sizeof(float), cudaMemcpyHostToDevice));
-    {
-        // One partial per 256-item block of every plane's padded range and per reduction row (level 0 is the wider
-        // unknown, so its texels bound every launch's block count).
-        size_t rblocks = 0;
-        for (const DevPlane& p : d->planes)
-            rblocks += ((size_t)p.w0 * p.h0 + THREADS - 1) / THREADS;
-        NB_ALLOC(d->partial, (size_t)RROWS * rblocks * sizeof(double));
-    }
-    NB_ALLOC(d->scalars, (size_t)MAX_PLANES * S_COUNT * sizeof(double));
     NB_CK(cudaMemset(d->scalars, 0, (size_t)MAX_PLANES * S_COUNT * sizeof(double)));
-    NB_ALLOC(d->counters, (size_t)COUNTERS * sizeof(unsigned int));
-    const int mm = m->nin + 1;
-    const size_t entries = (size_t)(mm * (mm + 1) / 2 + m->nout * mm);
-    NB_ALLOC(d->reduction, entries * sizeof(double));
-    NB_CK(cudaMemset(d->reduction, 0, entries * sizeof(double)));
-    NB_ALLOC(d->bc_stats, (size_t)MAX_PLANES * 2 * sizeof(double));
-    NB_ALLOC(d->radix, (size_t)std::max(2 * MAX_CH * 2048, MAX_NOUT * MAX_NOUT) * sizeof(unsigned int));
     {
-        // The assembly's per-site gradient terms: every site of every plane at the largest K (4), one double per channel
-        // of the wider unknown.
-        size_t sites = 0;
-        for (const DevPlane& p : d->planes)
-            sites += (size_t)p.w0 * p.h0 * 5;
-        d->site_terms_count = sites * (size_t)std::max(m->c0, m->c1);
-        NB_ALLOC(d->site_terms, d->site_terms_count * sizeof(double));
-        NB_ALLOC(d->site_y, sites * 4 * sizeof(float));
-        NB_ALLOC(d->gtab[0], (size_t)GATHER_TABLE_MAX * 16);
-        NB_ALLOC(d->gtab[1], (size_t)GATHER_TABLE_MAX * 16);
+        const int mm = m->nin + 1;
+        NB_CK(cudaMemset(d->reduction, 0, (size_t)(mm * (mm + 1) / 2 + m->nout * mm) * sizeof(double)));
     }
-    {
-        // The objective's partials: one triple per 256-pixel block of every plane, then the three sums per plane.
-        size_t blocks = 0;
-        for (const DevPlane& p : d->planes)
-            blocks += ((size_t)p.w0 * p.h0 + THREADS - 1) / THREADS;
-        // (the objective's 128-thread blocks: two partials per 256-pixel block)
-        NB_ALLOC(d->obj_partial, (2 * blocks * 3 + 3 * MAX_PLANES) * sizeof(double));
-    }
-    d->scratch_floats = std::max(max0 * (size_t)m->c0, max1 * (size_t)m->c1);
-    d->scratch_bytes = d->scratch_floats;
-    NB_ALLOC(d->scratch, d->scratch_floats * sizeof(float));
-    NB_ALLOC(d->scratch8, d->scratch_bytes);
-    NB_ALLOC(d->rgb8, max0 * m->nout);
-    NB_ALLOC(d->means, max1 * m->nout * sizeof(float));
-    if (m->init0_residual)
-        NB_ALLOC(d->resid, max0 * m->nout * sizeof(float));
     NB_CK(cudaMallocHost(&d->host_scalars, (size_t)MAX_PLANES * S_COUNT * sizeof(double)));
     NB_CK(cudaMallocHost(&d->host_counters, (size_t)COUNTERS * sizeof(unsigned int)));
     // the set-up's copies and clears went to the legacy stream; the model's own stream does not wait for it
     NB_CK(cudaDeviceSynchronize());
     d->m.has_decoder = 0;
-#undef NB_ALLOC
 #undef NB_CK
     *out = d;
     return NNTC_B200_OK;
@@ -640,35 +680,7 @@ void nntc_b200_device_destroy(nntc_b200_device* d)
         return;
     if (d->stream)
         cudaStreamSynchronize(d->stream);
-    for (DevPlane& p : d->planes)
-    {
-        cudaFree(p.src);
-        cudaFree(p.v0);
-        cudaFree(p.v1);
-        cudaFree(p.k0);
-        cudaFree(p.k1);
-        for (Work& w : p.work)
-        {
-            cudaFree(w.stencil);
-            cudaFree(w.grad);
-            cudaFree(w.precond);
-            cudaFree(w.x);
-            cudaFree(w.r);
-            cudaFree(w.z);
-            cudaFree(w.p);
-            cudaFree(w.ap);
-            cudaFree(w.prev);
-        }
-        cudaFree(p.bc_ep);
-        cudaFree(p.bc_sel);
-    }
-    void* bufs[] = { d->weights, d->bias,     d->palette,   d->lo1,      d->hi1,         d->lo0,
-                     d->hi0,     d->cw,       d->mono[0],   d->mono[1],  d->partial,     d->scalars,
-                     d->counters, d->reduction, d->ls_partial, d->obj_partial, d->bc_stats, d->resid, d->site_terms,
-                     d->site_y,    d->gtab[0],   d->gtab[1],  d->radix,
-                     d->means,   d->cov,      d->hist,      d->scratch,  d->scratch8,    d->rgb8 };
-    for (void* b : bufs)
-        cudaFree(b);
+    cudaFree(d->arena);
     cudaFreeHost(d->host_scalars);
     cudaFreeHost(d->host_counters);
     for (const nntc_b200_device::Pending& p : d->kpending)

@@ -48,6 +48,9 @@ constexpr int RGRID = 148 * 4;
 constexpr int RROWS = 3 + 2 * MAX_CH;
 constexpr int THREADS = 256;
 constexpr int GATHER_TABLE_MAX = 8192;   // int4 entries of one visit table
+constexpr int LS_GRID = 148 * 4;         // normal equations: blocks per plane (four per SM at the base plane)
+constexpr int COV_GRID = 512;            // init covariance: partials per entry
+constexpr int HIST_BINS = 4096;          // init0: the percentile histogram
 // The counter words: the quantised sweeps' moved count per plane, block (c)'s four colour passes per plane, and the
 // conjugate gradients' active-plane counts of the last CG_PROBE iterations.
 constexpr int CNT_SWEEP = 0;
@@ -108,7 +111,7 @@ struct nntc_b200_device
     double* scalars = nullptr;           // MAX_PLANES * S_COUNT
     unsigned int* counters = nullptr;    // COUNTERS words
     double* reduction = nullptr;         // the normal equations of the last block (a)
-    double* ls_partial = nullptr;        // entries * LS_GRID
+    double* ls_partial = nullptr;        // planes * entries * LS_GRID, then one weight per plane
     double* obj_partial = nullptr;       // 3 * MAX_PLANES * OBJ_GRID
     double* bc_stats = nullptr;          // MAX_PLANES * 2
     unsigned int* radix = nullptr;       // 2 * MAX_CH * 2048 words: the grid fit's histograms and flags
@@ -131,7 +134,9 @@ struct nntc_b200_device
     cudaEvent_t ev[4] = {};
     double* host_scalars = nullptr;      // pinned, MAX_PLANES * S_COUNT
     unsigned int* host_counters = nullptr;
-    size_t bytes = 0;
+    void* arena = nullptr;               // the one device allocation every buffer above is a slice of
+    void* keep = nullptr;                // bc8: the outer repack loop's copy of both latents and the BC state
+    size_t bytes = 0;                    // the arena's size
     int nout = 0, nin = 0, c0 = 0, c1 = 0;
     bool l0_bc8 = false;
 
@@ -151,6 +156,26 @@ struct nntc_b200_device
 
 namespace nb
 {
+
+// What the outer repack loop keeps of a rejected pass (bc8): both latents' values and indices and the BC state of
+// every plane, each part at a 256-byte boundary of the device's `keep` buffer.
+template <typename F>
+void for_each_kept(nntc_b200_device* d, F f)
+{
+    for (DevPlane& p : d->planes)
+    {
+        const size_t n0 = (size_t)p.w0 * p.h0 * d->c0, n1 = (size_t)p.w1 * p.h1 * d->c1;
+        f((void*)p.v0, n0 * sizeof(float));
+        f((void*)p.k0, n0);
+        f((void*)p.v1, n1 * sizeof(float));
+        f((void*)p.k1, n1);
+        if (d->l0_bc8)
+        {
+            f((void*)p.bc_ep, p.blocks() * d->c0 * 2);
+            f((void*)p.bc_sel, p.blocks() * d->c0 * 16);
+        }
+    }
+}
 
 // The Planes descriptor of a call, with the per-plane item ranges padded to whole THREADS-sized chunks so that no
 // chunk of a launch straddles two planes. `items(i)` is the plane's work-item count.

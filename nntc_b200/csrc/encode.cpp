@@ -23,53 +23,28 @@ namespace
 
 constexpr double E_REL = 1e-6, E_NOISE = 1e-8;   // src/main.cpp:371-372 (the rise warning, not a decision)
 
-// Both latents' planes, indices and BC state of every plane, copied device to device: what the outer repack loop
-// restores when a pass does not lower the shipped E.
-struct DeviceCopy
+// Both latents' planes, indices and BC state of every plane, copied device to device into the device's `keep`
+// slice: what the outer repack loop restores when a pass does not lower the shipped E.
+int snapshot(nntc_b200_device* d, bool save)
 {
-    void* buf = nullptr;
-    size_t bytes = 0;
-    ~DeviceCopy()
+    if (!d->keep)
     {
-        if (buf)
-            cudaFree(buf);
-    }
-};
-
-int snapshot(nntc_b200_device* d, DeviceCopy& keep, bool save)
-{
-    std::vector<std::pair<void*, size_t>> parts;
-    for (nb::DevPlane& p : d->planes)
-    {
-        const size_t n0 = (size_t)p.w0 * p.h0 * d->c0, n1 = (size_t)p.w1 * p.h1 * d->c1;
-        parts.push_back({ p.v0, n0 * sizeof(float) });
-        parts.push_back({ p.k0, n0 });
-        parts.push_back({ p.v1, n1 * sizeof(float) });
-        parts.push_back({ p.k1, n1 });
-        if (p.bc_ep)
-        {
-            parts.push_back({ p.bc_ep, p.blocks() * d->c0 * 2 });
-            parts.push_back({ p.bc_sel, p.blocks() * d->c0 * 16 });
-        }
-    }
-    size_t total = 0;
-    for (auto& q : parts)
-        total += (q.second + 255) / 256 * 256;
-    if (!keep.buf)
-    {
-        NB_CUDA(cudaMalloc(&keep.buf, total));
-        keep.bytes = total;
+        nb::set_error(NNTC_B200_ERR_STATE, "the outer repack loop runs only under --l0 bc8");
+        return NNTC_B200_ERR_STATE;
     }
     size_t at = 0;
-    for (auto& q : parts)
-    {
-        char* slot = (char*)keep.buf + at;
-        if (save)
-            NB_CUDA(cudaMemcpyAsync(slot, q.first, q.second, cudaMemcpyDeviceToDevice, d->stream));
-        else
-            NB_CUDA(cudaMemcpyAsync(q.first, slot, q.second, cudaMemcpyDeviceToDevice, d->stream));
-        at += (q.second + 255) / 256 * 256;
-    }
+    int st = NNTC_B200_OK;
+    nb::for_each_kept(d, [&](void* part, size_t bytes) {
+        char* slot = (char*)d->keep + at;
+        at += (bytes + 255) / 256 * 256;
+        if (st != NNTC_B200_OK || bytes == 0)
+            return;
+        const cudaError_t e = save ? cudaMemcpyAsync(slot, part, bytes, cudaMemcpyDeviceToDevice, d->stream)
+                                   : cudaMemcpyAsync(part, slot, bytes, cudaMemcpyDeviceToDevice, d->stream);
+        if (e != cudaSuccess)
+            st = nb::cuda_status(e, "cudaMemcpyAsync", __FILE__, __LINE__);
+    });
+    NB_TRY(st);
     NB_CUDA(cudaStreamSynchronize(d->stream));
     return NNTC_B200_OK;
 }
@@ -366,11 +341,10 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             NB_TRY(objective(probe));
         }
         double e_ship = probe.e;
-        DeviceCopy keep;
         for (int pass = 1; pass <= a->bc_outer; pass++)
         {
             // Everything a rejected pass would leave behind, kept on the device (src/main.cpp:2561-2590).
-            NB_TRY(snapshot(d, keep, true));
+            NB_TRY(snapshot(d, true));
             const nntc_b200_model keep_m = *m;
             NB_TRY(refit_level1());
             NB_TRY(block_a());
@@ -393,7 +367,7 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
                 r->outer_taken++;
                 continue;
             }
-            NB_TRY(snapshot(d, keep, false));
+            NB_TRY(snapshot(d, false));
             *m = keep_m;
             NB_TRY(nntc_b200_upload_decoder(d, m));
             NB_TRY(nntc_b200_upload_grids(d, m));

@@ -22,7 +22,6 @@
 namespace nb
 {
 
-constexpr int COV_GRID = 512;
 
 struct ChannelBits
 {
@@ -365,8 +364,6 @@ static void jacobi_eigen(std::vector<double>& a, int n, std::vector<double>& vec
 static int cov_sums(nntc_b200_device* d, const float* rows, size_t count, int nout, std::vector<double>& raw)
 {
     const int entries = nout + nout * nout;
-    if (!d->cov)
-        NB_CUDA(cudaMalloc(&d->cov, (size_t)(MAX_NOUT + MAX_NOUT * MAX_NOUT) * COV_GRID * sizeof(double)));
     dim3 grid((unsigned)COV_GRID, (unsigned)nout);
     k_cov_partial<<<grid, 256, 0, d->stream>>>(rows, count, nout, d->cov);
     NB_LAUNCHED();
@@ -681,8 +678,6 @@ int nntc_b200_init0_residual_channel(nntc_b200_device* d, const nntc_b200_model*
         rep->dir[r] = dir.e[r];
 
     double peak = 0.0;
-    if (!d->cov)
-        NB_CUDA(cudaMalloc(&d->cov, (size_t)(MAX_NOUT + MAX_NOUT * MAX_NOUT) * COV_GRID * sizeof(double)));
     std::vector<double> partial((size_t)COV_GRID, 0.0);
     for (size_t i = 0; i < d->planes.size(); i++)
     {
@@ -698,11 +693,9 @@ int nntc_b200_init0_residual_channel(nntc_b200_device* d, const nntc_b200_model*
     rep->peak = peak;
     rep->divisor = peak;
     double divisor = peak;
-    const int BINS = 4096;
+    const int BINS = HIST_BINS;
     if (!m->l0_bc8 && peak > 0.0)
     {
-        if (!d->hist)
-            NB_CUDA(cudaMalloc(&d->hist, BINS * sizeof(unsigned long long)));
         NB_CUDA(cudaMemsetAsync(d->hist, 0, BINS * sizeof(unsigned long long), d->stream));
         unsigned long long total = 0ull;
         for (size_t i = 0; i < d->planes.size(); i++)
