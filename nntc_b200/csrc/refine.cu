@@ -292,19 +292,6 @@ __device__ __forceinline__ double row_of(const double (&uv)[R], int idx)
     return v;
 }
 
-// The same for an idx every lane holds alike: the slot it sits in is then the same on every lane too, so only that
-// slot is shuffled.
-template <int R>
-__device__ __forceinline__ double row_of_uniform(const double (&uv)[R], int idx)
-{
-    double x = uv[0];
-#pragma unroll
-    for (int q = 1; q < R; q++)
-        if ((idx >> 5) == q)
-            x = uv[q];
-    return __shfl_sync(0xffffffffu, x, idx & 31);
-}
-
 // The sixteen lanes' terms folded serially in texel order, the same on every lane.
 __device__ __forceinline__ double fold16(double v)
 {
@@ -556,16 +543,23 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
     // Every group of eight lanes evaluates the eight candidates, one per lane, and takes the lowest change in three
     // butterfly rounds, ties to the lower candidate: the candidate the reference's in-order scan with a strict `<`
     // keeps, and no candidate when none lowers E.
-    const int k8 = lane & 7;
+    //
+    // The four groups of eight lanes take four consecutive texels' steps at once, each against the current u. A step's
+    // inputs are the sequential scan's as long as no earlier step of the four moved a selector; so the first step of
+    // the four that lowers E is taken, the steps before it stand (none of them lowered E), and the scan resumes after
+    // it. Steps that lower nothing, the common case once the selectors settle, cost a quarter of an iteration each.
+    const int k8 = lane & 7, grp = lane >> 3;
     for (int pass = 0; pass < 2; pass++)
         for (int c = 0; c < C0; c++)
         {
             const int r0 = s_ep[2 * c], r1 = s_ep[2 * c + 1];
             const double cand = (double)bc0_value(R.lo0[c], R.hi0[c], bc4_entry(r0, r1, k8));
-            for (int t = 0; t < 16; t++)
+            int t0 = 0;
+            while (t0 < 16)
             {
+                const int t = t0 + grp < 16 ? t0 + grp : 15;   // past the last texel a group repeats it, unused
                 const int i = t * C0 + c;
-                const double b = a1[i] + row_of_uniform(uv, i);
+                const double b = a1[i] + row_of(uv, i);
                 const double a = S[t * TS + c * C0 + c];
                 const int cur = s_sel[c * 16 + t];
                 const double now = __shfl_sync(0xffffffffu, cand, cur);
@@ -579,28 +573,36 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
 #pragma unroll
                 for (int o = 1; o < 8; o <<= 1)
                     v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-                const unsigned hits = __ballot_sync(0xffffffffu, lane < 8 && mine == v);
-                const int id = __ffs(hits) - 1;
-                const double mv = __shfl_sync(0xffffffffu, d, id & 7);
-                // v, mv and id are the same on every lane
-                if (v < 0.0)
+                const unsigned hits = __ballot_sync(0xffffffffu, mine == v);
+                const int id = __ffs((hits >> (grp * 8)) & 0xffu) - 1;
+                const unsigned lowers = __ballot_sync(0xffffffffu, k8 == 0 && t0 + grp < 16 && v < 0.0);
+                if (lowers == 0u)
                 {
-#pragma unroll
-                    for (int q = 0; q < RR; q++)
-                    {
-                        const int r = lane + 32 * q;
-                        if (r >= N)
-                            continue;
-                        const int rt = r / C0, ri = r % C0;
-                        const int k = neighbour_index(rt, t);
-                        if (k >= 0)
-                            uv[q] += a2_entry<C0>(S, rt, ri, t, c, k) * mv;
-                    }
-                    if (lane == 0)
-                        s_sel[c * 16 + t] = (unsigned char)id;
-                    taken += v;
+                    t0 += 4;
+                    continue;
                 }
+                // the first group whose step lowers E: its texel, change, candidate and new value on every lane
+                const int g = (__ffs(lowers) - 1) >> 3;
+                const int tf = t0 + g;
+                const double vf = __shfl_sync(0xffffffffu, v, g * 8);
+                const int idf = __shfl_sync(0xffffffffu, id, g * 8);
+                const double mv = __shfl_sync(0xffffffffu, d, g * 8 + idf);
+#pragma unroll
+                for (int q = 0; q < RR; q++)
+                {
+                    const int r = lane + 32 * q;
+                    if (r >= N)
+                        continue;
+                    const int rt = r / C0, ri = r % C0;
+                    const int k = neighbour_index(rt, tf);
+                    if (k >= 0)
+                        uv[q] += a2_entry<C0>(S, rt, ri, tf, c, k) * mv;
+                }
+                if (lane == 0)
+                    s_sel[c * 16 + tf] = (unsigned char)idf;
+                taken += vf;
                 __syncwarp();
+                t0 = tf + 1;
             }
         }
 
