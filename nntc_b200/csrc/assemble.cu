@@ -44,6 +44,13 @@ __host__ __device__ constexpr int pair_k(int p)
     return p < 4 ? p : (p < 7 ? p - 3 : (p < 9 ? p - 5 : 3));
 }
 
+// Whether slot L of the fixed monomial layout (the constant, four linear terms, ten products) is a monomial of a
+// latent with ny channels: the used slots, in slot order, are the reference's monomials in its order.
+__host__ __device__ constexpr bool mono_used(int L, int ny)
+{
+    return L == 0 || (L <= MAX_CH ? L - 1 < ny : pair_k(L - 5) < ny);
+}
+
 struct SiteArgs
 {
     double* terms;                      // [site][c] over every plane
@@ -308,10 +315,11 @@ struct GatherArgs
 {
     const double* terms;
     const float4* y;      // [site]: the site's sample of the other latent, from k_site_terms
-    const double* mono;   // nmono matrices of c x c
+    // the monomial matrices (c x c, row-major) at their monomial's slot of the fixed layout, unused slots left out:
+    // with the expansion unrolled every entry is a constant-bank operand, no loads
+    double mono[MAX_MONO][MAX_CH * MAX_CH];
     const int4* tab;      // the visit tables of this level and K
     GatherTable gt;
-    int nmono;
     unsigned tabled;      // bit i: plane i's interior texels may use the tables
     long long site0[MAX_PLANES + 1];
     long long bstart[MAX_PLANES + 1];   // each plane's first block
@@ -351,7 +359,7 @@ __device__ __forceinline__ void stencil_texel(long long pos, int w, int h, int& 
 // take the texels in the stencil's colour-major order, so a warp's texels share a parity class (one visit table) and
 // its stores are contiguous.
 template <bool LEVEL0>
-__global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs A)
+__global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, const __grid_constant__ GatherArgs A)
 {
     // Block order: (region, colour, slot) with the slot fastest. The five slots of one run of texels, and the four
     // colours of one region of the plane, are consecutive blocks, so they run side by side and share the region's sites
@@ -374,7 +382,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
         return;
     // the texel's place in the stencil's colour-major order
     const long long sp = within + (colour == 0 ? 0 : (colour == 1 ? n0 : (colour == 2 ? n0 + n1 : n0 + n1 + n2)));
-    const int c0 = P.c0, c1 = P.c1, kc = P.kc, per = 1 + kc, nmono = A.nmono;
+    const int c0 = P.c0, c1 = P.c1, kc = P.kc, per = 1 + kc;
     const int c = LEVEL0 ? c0 : c1;
     int tx, ty;
     stencil_texel(sp, tw_, th_, tx, ty);
@@ -501,22 +509,18 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
 #pragma unroll
     for (int e = 0; e < MAX_CH * MAX_CH; e++)
         blk[e] = 0.0;
-    int q = 0;
 #pragma unroll
     for (int L = 0; L < MAX_MONO; L++)
     {
-        const bool valid = L == 0 || (L <= MAX_CH ? L - 1 < ny_ : pair_k(L - 5) < ny_);
-        if (!valid)
+        if (!mono_used(L, ny_))
             continue;
         const double s = sums[L];
-        const double* mat = A.mono + (size_t)q * cc;
-        q++;
         if (s == 0.0)
             continue;
 #pragma unroll
         for (int e = 0; e < MAX_CH * MAX_CH; e++)
             if (e < cc)
-                blk[e] += s * __ldg(mat + e);
+                blk[e] += s * A.mono[L][e];
     }
 #pragma unroll
     for (int e = 0; e < MAX_CH * MAX_CH; e++)
@@ -532,7 +536,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, GatherArgs 
 }
 
 // Launch both passes for every plane: the per-site terms, then the per-(texel, slot) gather.
-int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono)
+int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono)
 {
     Planes S = planes_for(d, level0, [&](int i) {
         const DevPlane& p = d->planes[(size_t)i];
@@ -543,8 +547,21 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     GatherArgs G{};
     G.terms = d->site_terms;
     G.y = (const float4*)d->site_y;
-    G.mono = d->mono[level0];
-    G.nmono = nmono;
+    {
+        const int ny = level0 ? d->c1 : d->c0, c = level0 ? d->c0 : d->c1;
+        int q = 0;
+        for (int L = 0; L < MAX_MONO; L++)
+            if (mono_used(L, ny))
+            {
+                std::memcpy(G.mono[L], mono + (size_t)q * c * c, (size_t)c * c * sizeof(double));
+                q++;
+            }
+        if (q != nmono)
+        {
+            set_error(NNTC_B200_ERR_STATE, "monomial layout and count disagree");
+            return NNTC_B200_ERR_STATE;
+        }
+    }
     if (d->gtab_kc[level0] != k)
     {
         std::vector<int4> tab;

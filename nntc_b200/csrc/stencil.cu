@@ -974,7 +974,7 @@ static Red red_for(nntc_b200_device* d, const Planes& P)
     return Red{ d->partial, (size_t)(P.start[P.n] / THREADS), d->scalars };
 }
 
-int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono);
+int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono);
 
 int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0)
 {
@@ -993,7 +993,7 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
     AsmArgs A{ d->weights, d->bias, d->cw, d->mono[level0], nmono };
     NB_TRY(ktimer_begin(d, level0 ? NNTC_B200_K_ASSEMBLE0 : NNTC_B200_K_ASSEMBLE1));
     if (!d->reference_shaped_assembly && k <= 4)
-        NB_TRY(assemble_split(d, k, level0, P, nmono));
+        NB_TRY(assemble_split(d, k, level0, P, nmono, mono.data()));
     else if (level0)
     {
         NB_CUDA(cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
