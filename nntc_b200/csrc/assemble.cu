@@ -359,7 +359,7 @@ __device__ __forceinline__ void stencil_texel(long long pos, int w, int h, int& 
 // take the texels in the stencil's colour-major order, so a warp's texels share a parity class (one visit table) and
 // its stores are contiguous.
 template <bool LEVEL0>
-__global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, const __grid_constant__ GatherArgs A)
+__device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A)
 {
     // Block order: (region, colour, slot) with the slot fastest. The five slots of one run of texels, and the four
     // colours of one region of the plane, are consecutive blocks, so they run side by side and share the region's sites
@@ -504,35 +504,62 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather(Planes P, const __gri
                 }
     }
 
-    // the slot's block, expanded once against the monomial matrices in the reference's order (src/solve_level1.cu:382-399)
-    double blk[MAX_CH * MAX_CH];
+    // the slot's block, expanded once against the monomial matrices in the reference's order (src/solve_level1.cu:382-399);
+    // level 1 expands it in two halves of eight entries (each entry's own sum still in monomial order) so that fewer
+    // doubles are live at once and seven blocks fit an SM
+    // (where the gradient's store goes changes only which registers are live when: each level's place is the one that
+    // spills least at its occupancy)
+    auto store_grad = [&]() {
+        if (slot == 0)
+        {
 #pragma unroll
-    for (int e = 0; e < MAX_CH * MAX_CH; e++)
-        blk[e] = 0.0;
+            for (int a = 0; a < MAX_CH; a++)
+                if (a < c)
+                    V.grad[ti * c + a] = g[a];
+        }
+    };
+    if (!LEVEL0)
+        store_grad();
+    constexpr int PART = LEVEL0 ? MAX_CH * MAX_CH : 8;
 #pragma unroll
-    for (int L = 0; L < MAX_MONO; L++)
+    for (int part = 0; part < MAX_CH * MAX_CH / PART; part++)
     {
-        if (!mono_used(L, ny_))
-            continue;
-        const double s = sums[L];
-        if (s == 0.0)
-            continue;
+        double blk[PART];
 #pragma unroll
-        for (int e = 0; e < MAX_CH * MAX_CH; e++)
-            if (e < cc)
-                blk[e] += s * A.mono[L][e];
+        for (int e = 0; e < PART; e++)
+            blk[e] = 0.0;
+#pragma unroll
+        for (int L = 0; L < MAX_MONO; L++)
+        {
+            if (!mono_used(L, ny_))
+                continue;
+            const double s = sums[L];
+            if (s == 0.0)
+                continue;
+#pragma unroll
+            for (int e = 0; e < PART; e++)
+                if (part * PART + e < cc)
+                    blk[e] += s * A.mono[L][part * PART + e];
+        }
+#pragma unroll
+        for (int e = 0; e < PART; e++)
+            if (part * PART + e < cc)
+                V.stencil[(size_t)(slot * cc + part * PART + e) * T + sp] = blk[e];
     }
-#pragma unroll
-    for (int e = 0; e < MAX_CH * MAX_CH; e++)
-        if (e < cc)
-            V.stencil[(size_t)(slot * cc + e) * T + sp] = blk[e];
-    if (slot == 0)
-    {
-#pragma unroll
-        for (int a = 0; a < MAX_CH; a++)
-            if (a < c)
-                V.grad[ti * c + a] = g[a];
-    }
+    if (LEVEL0)
+        store_grad();
+}
+
+// The two levels' kernels: level 1 capped at seven blocks per SM (its expansion is split for that), level 0 left at
+// the register count it takes unconstrained (a cap made it spill and run slower).
+__global__ void __launch_bounds__(GATHER_THREADS) k_gather_level0(Planes P, const __grid_constant__ GatherArgs A)
+{
+    gather_body<true>(P, A);
+}
+
+__global__ void __launch_bounds__(GATHER_THREADS, 7) k_gather_level1(Planes P, const __grid_constant__ GatherArgs A)
+{
+    gather_body<false>(P, A);
 }
 
 // Launch both passes for every plane: the per-site terms, then the per-(texel, slot) gather.
@@ -644,9 +671,9 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     G.bstart[P_texels.n] = blocks;
     const unsigned grid = (unsigned)blocks;
     if (level0)
-        k_gather<true><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+        k_gather_level0<<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
     else
-        k_gather<false><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+        k_gather_level1<<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
     NB_LAUNCHED();
     return NNTC_B200_OK;
 }
