@@ -326,11 +326,11 @@ def main():
 # the CG matvec), from one ncu capture (--set full) of the 4 x 2048 x 1024 material; a launch's traffic grows with the
 # pixels it covers, so the bench scales these to its own workload.
 TRAFFIC_PER_UNIT = {
-    "assemble_level0": (800033000 + 2499623000) / 2796160,   # k_site_terms<1> + k_gather<1>
-    "assemble_level1": (795370000 + 1370403000) / 2796160,   # k_site_terms<0> + k_gather<0>
+    "assemble_level0": (796251000 + 2499329000) / 2796160,   # k_site_terms<1> + k_gather_level0
+    "assemble_level1": (797819000 + 1779162000) / 2796160,   # k_site_terms<0> + k_gather_level1
     "objective": 186521344 / 2796160,
     "normal_equations": 187554048 / 2796160,
-    "bc_refine": 1194284328 / 2796160,                       # one colour
+    "bc_refine": 1193938312 / 2796160,                       # one colour
 }
 
 # What bounds each group, from the same captures: the roofline the HBM fraction alone does not show.
@@ -339,7 +339,7 @@ BINDING = {
     "assemble_level1": "FP32/ALU issue (site terms) and L2 latency (gather); FP64 compute, not HBM",
     "objective": "FP64 pipe (~50% of peak)",
     "normal_equations": "FP64 tensor pipe and site staging",
-    "bc_refine": "latency of 128 ordered selector steps per block",
+    "bc_refine": "latency: the set-up's scattered stencil reads, then the ordered selector steps (four evaluated at once)",
     "quant_sweep": "HBM (level-0 colour launch ~79% of measured copy bandwidth)",
     "cg_matvec": "HBM",
 }
