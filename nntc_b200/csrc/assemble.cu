@@ -55,8 +55,48 @@ struct SiteArgs
 {
     double* terms;                      // [site][c] over every plane
     float4* y;                          // [site]: the site's sample of the other latent
+    const float* tgt;                   // [fractional site][NOUT]: the targets of the sites j > 0 (k_site_targets)
     long long site0[MAX_PLANES + 1];    // the first site of each plane in `terms`
+    long long tsite0[MAX_PLANES + 1];   // the first fractional site of each plane in `tgt`
 };
+
+struct TargetOffsets
+{
+    long long site0[MAX_PLANES + 1];    // the first fractional site of each plane
+};
+
+// The float target of every fractional site (j > 0): the source blended at the site's four level-0 taps, in blend()'s
+// order and arithmetic (src/solve_level1.cu:322-333). It depends on nothing but the source and K, neither of which an
+// encode changes, so it is formed once per device model and K and then read by every k_site_terms launch.
+template <int NOUT>
+__global__ void __launch_bounds__(SITE_THREADS) k_site_targets(Planes P, float* tgt, const __grid_constant__ TargetOffsets O)
+{
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long fi = base - P.start[pl] + threadIdx.x;
+    const int kc = P.kc;
+    if (fi >= (long long)V.w0 * V.h0 * kc)
+        return;
+    const long long pixel = fi / kc;
+    const int j = 1 + (int)(fi % kc);
+    const int px = (int)(pixel % V.w0), py = (int)(pixel / V.w0);
+    float dx, dy;
+    site_offset(kc, j, px, py, dx, dy);
+    const Tap t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+    float w0[4];
+    tap_weights(t0, w0);
+    float* out = tgt + (size_t)(O.site0[pl] + fi) * NOUT;
+#pragma unroll
+    for (int r = 0; r < NOUT; r++)
+    {
+        const float* s = V.src + r;
+        out[r] = w0[0] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x0) * NOUT) +
+                 w0[1] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x1) * NOUT) +
+                 w0[2] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x0) * NOUT) +
+                 w0[3] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x1) * NOUT);
+    }
+}
 
 // One thread per site: t_s[a] = sum_r cw_r G[r][a] res_r (level 1, block b) or sum_r cw_r Q[r][a] res_r (level 0,
 // block c'), in the reference's order of operations (src/solve_level1.cu:335-361, 518-544).
@@ -89,8 +129,6 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
     float sbar[MAX_CH], cbar[MAX_CH];
     const Tap tp = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
     blend_u<MAX_CH>(V.v1, V.w1, c1, tp, cbar);
-    Tap t0{};
-    float w0[4];
     if (j == 0)
     {
 #pragma unroll
@@ -100,10 +138,11 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
     }
     else
     {
-        t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
+        const Tap t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
         blend_u<MAX_CH>(V.v0, V.w0, c0, t0, sbar);
-        tap_weights(t0, w0);
     }
+    // the targets: the pixel's own source at the centre site, else the fractional site's blend from k_site_targets
+    const float* tgt = j > 0 ? A.tgt + (size_t)(A.tsite0[pl] + pixel * kc + (j - 1)) * NOUT : V.src + pixel * NOUT;
     double acc[MAX_CH];
 #pragma unroll
     for (int a = 0; a < MAX_CH; a++)
@@ -111,18 +150,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
 #pragma unroll
     for (int r = 0; r < NOUT; r++)
     {
-        // the target of this output, sampled as blend() samples it
-        float target;
-        if (j == 0)
-            target = __ldg(V.src + pixel * NOUT + r);
-        else
-        {
-            const float* s = V.src + r;
-            target = w0[0] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x0) * NOUT) +
-                     w0[1] * __ldg(s + ((size_t)t0.y0 * V.w0 + t0.x1) * NOUT) +
-                     w0[2] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x0) * NOUT) +
-                     w0[3] * __ldg(s + ((size_t)t0.y1 * V.w0 + t0.x1) * NOUT);
-        }
+        const float target = __ldg(tgt + r);
         const float* row = W.w + r * 24;   // [c_q][s_i][s_i c_q]
         float out = W.b[r];
         float col[MAX_CH];
@@ -624,6 +652,46 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
         at += (long long)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0 * (1 + k);
     }
     A.site0[S.n] = G.site0[S.n] = at;
+    // the fractional sites' targets, formed on the first assembly at this K
+    A.tgt = d->site_tgt;
+    {
+        TargetOffsets O{};
+        long long ft = 0;
+        for (int i = 0; i < S.n; i++)
+        {
+            O.site0[i] = A.tsite0[i] = ft;
+            ft += (long long)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0 * k;
+        }
+        O.site0[S.n] = A.tsite0[S.n] = ft;
+        if (d->site_tgt_kc != k && k > 0)
+        {
+            Planes T = planes_for(d, level0, [&](int i) {
+                const DevPlane& p = d->planes[(size_t)i];
+                return (size_t)p.w0 * p.h0 * (size_t)k;
+            });
+            T.kc = k;
+            const int tblocks = (int)(T.start[T.n] / SITE_THREADS);
+#define NB_TARGETS(NO)                                                                                                \
+    case NO:                                                                                                          \
+        k_site_targets<NO><<<tblocks, SITE_THREADS, 0, d->stream>>>(T, d->site_tgt, O);                               \
+        break;
+            switch (d->nout)
+            {
+                NB_TARGETS(3)
+                NB_TARGETS(6)
+                NB_TARGETS(9)
+                NB_TARGETS(12)
+                NB_TARGETS(15)
+                NB_TARGETS(18)
+            default:
+                set_error(NNTC_B200_ERR_STATE, "a material holds 1..6 RGB textures");
+                return NNTC_B200_ERR_STATE;
+            }
+#undef NB_TARGETS
+            NB_LAUNCHED();
+        }
+        d->site_tgt_kc = k;
+    }
     const int sblocks = (int)(S.start[S.n] / SITE_THREADS);
     SiteDecoder W{};
     const int nin = d->nin, c0 = d->c0, c1 = d->c1;

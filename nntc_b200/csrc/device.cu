@@ -363,6 +363,8 @@ void layout(nntc_b200_device* d, const nntc_b200_model* m, Carver& take)
     d->site_terms_count = sites * (size_t)std::max(m->c0, m->c1);
     take(d->site_terms, d->site_terms_count * sizeof(double));
     take(d->site_y, sites * 4 * sizeof(float));
+    take(d->site_tgt, sites / 5 * 4 * m->nout * sizeof(float));   // four fractional sites per pixel at K = 4
+    take(d->obj_tgt, sites / 5 * 4 * m->nout * sizeof(double));
     take(d->gtab[0], (size_t)GATHER_TABLE_MAX * 16);
     take(d->gtab[1], (size_t)GATHER_TABLE_MAX * 16);
     // the objective's partials: two triples per 256-pixel block (its blocks are 128 threads), then three sums per plane

@@ -118,6 +118,10 @@ struct nntc_b200_device
     double* site_terms = nullptr;        // every site's gradient term of the assembly, max(C0, C1) per site at K = 4
     size_t site_terms_count = 0;         // doubles in site_terms
     float* site_y = nullptr;             // every site's sample of the OTHER latent, 4 floats per site (assembly)
+    float* site_tgt = nullptr;           // the fractional sites' float targets at K, nout per site (assembly)
+    int site_tgt_kc = -1;                // the K site_tgt holds (-1: none yet; the source never changes)
+    double* obj_tgt = nullptr;           // the fractional sites' double targets at K, nout per site (objective)
+    int obj_tgt_kc = -1;                 // the K obj_tgt holds (-1: none yet)
     void* gtab[2] = { nullptr, nullptr };// the gather's visit tables of level 1 / level 0 (GATHER_TABLE_MAX int4 each)
     int gtab_kc[2] = { -1, -1 };         // the K each table was built for (-1: none yet)
     int gtab_off[2][4][6] = {};          // each table's entry ranges per parity class and slot

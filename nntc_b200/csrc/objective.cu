@@ -218,10 +218,55 @@ struct ObjDecoder
     double cw[MAX_NOUT];
 };
 
-// k_objective for a material of NOUT outputs (3 per texture), the decoder in the launch's parameters. The same sites,
-// the same operations in the same order, so the same bits as k_objective.
+// The target of every fractional site (j > 0) in double: the source's bilinear sample at the site as k_objective_p
+// took it inline, a chain of fused multiply-adds (a measurement: its last bits move, within the objective's 1e-12). It
+// depends on nothing but the source and K, neither of which an encode changes, so it is formed once per device model
+// and K and read by every later objective pass.
+struct ObjTargets
+{
+    const double* t;                   // [fractional site][NOUT]
+    long long site0[MAX_PLANES + 1];   // the first fractional site of each plane
+};
+
 template <int NOUT>
-__global__ void __launch_bounds__(OBJ_P_THREADS, 5) k_objective_p(Planes P, ObjDecoder W, double* partial)
+__global__ void __launch_bounds__(OBJ_THREADS) k_objective_targets(Planes P, double* tgt, const __grid_constant__ ObjTargets O)
+{
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long fi = base - P.start[pl] + threadIdx.x;
+    const int kc = P.kc;
+    if (fi >= (long long)V.w0 * V.h0 * kc)
+        return;
+    const long long local = fi / kc;
+    const int j = 1 + (int)(fi % kc);
+    const int px = (int)(local % V.w0), py = (int)(local / V.w0);
+    float dx = 0.0f, dy = 0.0f;
+    subtexel(kc, j - 1, px, py, dx, dy);
+    const double u = ((double)px + 0.5 + (double)dx) / (double)V.w0;
+    const double v = ((double)py + 0.5 + (double)dy) / (double)V.h0;
+    const double x = u * (double)V.w0 - 0.5, y = v * (double)V.h0 - 0.5;
+    const double xf = floor(x), yf = floor(y);
+    const double fx = x - xf, fy = y - yf;
+    const int x0 = clampi((int)xf, V.w0), x1 = clampi((int)xf + 1, V.w0);
+    const int y0 = clampi((int)yf, V.h0), y1 = clampi((int)yf + 1, V.h0);
+    const size_t ta = ((size_t)y0 * V.w0 + x0) * NOUT, tb = ((size_t)y0 * V.w0 + x1) * NOUT;
+    const size_t te = ((size_t)y1 * V.w0 + x0) * NOUT, tf = ((size_t)y1 * V.w0 + x1) * NOUT;
+    const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy), w01 = (1.0 - fx) * fy, w11 = fx * fy;
+    double* out = tgt + (size_t)(O.site0[pl] + fi) * NOUT;
+#pragma unroll
+    for (int r = 0; r < NOUT; r++)
+        out[r] = fma(w11, (double)__ldg(V.src + tf + r),
+                     fma(w01, (double)__ldg(V.src + te + r),
+                         fma(w10, (double)__ldg(V.src + tb + r), w00 * (double)__ldg(V.src + ta + r))));
+}
+
+// k_objective for a material of NOUT outputs (3 per texture), the decoder in the launch's parameters, the fractional
+// sites' targets from k_objective_targets. The same sites, the same operations in the same order as k_objective,
+// whose bits it matches but for the targets' fused multiply-adds.
+template <int NOUT>
+__global__ void __launch_bounds__(OBJ_P_THREADS, 5)
+    k_objective_p(Planes P, ObjDecoder W, double* partial, const __grid_constant__ ObjTargets T)
 {
     __shared__ double red[32];
     const int c0 = P.c0, c1 = P.c1, kc = P.kc;
@@ -248,8 +293,6 @@ __global__ void __launch_bounds__(OBJ_P_THREADS, 5) k_objective_p(Planes P, ObjD
                 c[q] = 0.0;
             }
             obj_sample<MAX_CH>(V.v1, V.w1, V.h1, c1, u, v, c);
-            size_t ta = (size_t)local * NOUT, tb = ta, te = ta, tf = ta;
-            double w00 = 1.0, w10 = 0.0, w01 = 0.0, w11 = 0.0;
             if (j == 0)
             {
 #pragma unroll
@@ -258,22 +301,7 @@ __global__ void __launch_bounds__(OBJ_P_THREADS, 5) k_objective_p(Planes P, ObjD
                         s[i] = (double)V.v0[local * c0 + i];
             }
             else
-            {
                 obj_sample<MAX_CH>(V.v0, V.w0, V.h0, c0, u, v, s);
-                const double x = u * (double)V.w0 - 0.5, y = v * (double)V.h0 - 0.5;
-                const double xf = floor(x), yf = floor(y);
-                const double fx = x - xf, fy = y - yf;
-                const int x0 = clampi((int)xf, V.w0), x1 = clampi((int)xf + 1, V.w0);
-                const int y0 = clampi((int)yf, V.h0), y1 = clampi((int)yf + 1, V.h0);
-                ta = ((size_t)y0 * V.w0 + x0) * NOUT;
-                tb = ((size_t)y0 * V.w0 + x1) * NOUT;
-                te = ((size_t)y1 * V.w0 + x0) * NOUT;
-                tf = ((size_t)y1 * V.w0 + x1) * NOUT;
-                w00 = (1.0 - fx) * (1.0 - fy);
-                w10 = fx * (1.0 - fy);
-                w01 = (1.0 - fx) * fy;
-                w11 = fx * fy;
-            }
             // every row's dot product advanced together, feature by feature (each row's own sum keeps phi's order),
             // so that NOUT independent chains of DFMAs are in flight at once; a product feature s_i c_q is formed
             // once, when its turn comes, instead of being held for the whole site
@@ -299,16 +327,13 @@ __global__ void __launch_bounds__(OBJ_P_THREADS, 5) k_objective_p(Planes P, ObjD
                 for (int r = 0; r < NOUT; r++)
                     acc[r] = fma(W.w[r * 24 + 8 + h], sc, acc[r]);
             }
+            // the pixel's own source at the centre site, else the fractional site's sample from k_objective_targets
+            const float* t_centre = V.src + (size_t)local * NOUT;
+            const double* t_frac = j > 0 ? T.t + (size_t)(T.site0[pl] + local * kc + (j - 1)) * NOUT : nullptr;
 #pragma unroll
             for (int r = 0; r < NOUT; r++)
             {
-                // the target's bilinear sample as a chain of fused multiply-adds (a measurement: its last bits move,
-                // within the objective's 1e-12)
-                const double t = j == 0 ? (double)__ldg(V.src + ta + r)
-                                        : fma(w11, (double)__ldg(V.src + tf + r),
-                                              fma(w01, (double)__ldg(V.src + te + r),
-                                                  fma(w10, (double)__ldg(V.src + tb + r),
-                                                      w00 * (double)__ldg(V.src + ta + r))));
+                const double t = j == 0 ? (double)__ldg(t_centre + r) : __ldg(t_frac + r);
                 const double e = acc[r] - t;
                 weighted = fma(W.cw[r] * e, e, weighted);
                 if (j == 0)
@@ -483,15 +508,47 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
         W.cw[r] = (double)d->m.cw[r];
     }
     NB_TRY(block_begin(d));
+    // the fractional sites' targets, formed on the first pass at this K
+    ObjTargets T{};
+    T.t = d->obj_tgt;
+    {
+        long long ft = 0;
+        for (int i = 0; i < P.n; i++)
+        {
+            T.site0[i] = ft;
+            ft += (long long)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0 * k;
+        }
+        T.site0[P.n] = ft;
+    }
+    if (d->obj_tgt_kc != k && k > 0 && bthreads == OBJ_P_THREADS)
+    {
+        Planes F = planes_for(d, 0, [&](int i) {
+            const DevPlane& p = d->planes[(size_t)i];
+            return (size_t)p.w0 * p.h0 * (size_t)k;
+        });
+        F.kc = k;
+        const int fblocks = (int)(F.start[F.n] / OBJ_THREADS);
+        switch (nout)
+        {
+        case 3: k_objective_targets<3><<<fblocks, OBJ_THREADS, 0, d->stream>>>(F, d->obj_tgt, T); break;
+        case 6: k_objective_targets<6><<<fblocks, OBJ_THREADS, 0, d->stream>>>(F, d->obj_tgt, T); break;
+        case 9: k_objective_targets<9><<<fblocks, OBJ_THREADS, 0, d->stream>>>(F, d->obj_tgt, T); break;
+        case 12: k_objective_targets<12><<<fblocks, OBJ_THREADS, 0, d->stream>>>(F, d->obj_tgt, T); break;
+        case 15: k_objective_targets<15><<<fblocks, OBJ_THREADS, 0, d->stream>>>(F, d->obj_tgt, T); break;
+        case 18: k_objective_targets<18><<<fblocks, OBJ_THREADS, 0, d->stream>>>(F, d->obj_tgt, T); break;
+        }
+        NB_LAUNCHED();
+        d->obj_tgt_kc = k;
+    }
     NB_TRY(ktimer_begin(d, NNTC_B200_K_OBJECTIVE));
     switch (nout)
     {
-    case 3: k_objective_p<3><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 6: k_objective_p<6><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 9: k_objective_p<9><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 12: k_objective_p<12><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 15: k_objective_p<15><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
-    case 18: k_objective_p<18><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial); break;
+    case 3: k_objective_p<3><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial, T); break;
+    case 6: k_objective_p<6><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial, T); break;
+    case 9: k_objective_p<9><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial, T); break;
+    case 12: k_objective_p<12><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial, T); break;
+    case 15: k_objective_p<15><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial, T); break;
+    case 18: k_objective_p<18><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, W, d->obj_partial, T); break;
     default:
         k_objective<<<nblocks, OBJ_THREADS, 0, d->stream>>>(P, ObjArgs{ d->weights, d->bias, d->cw, d->obj_partial });
     }
