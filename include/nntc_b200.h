@@ -40,7 +40,8 @@ enum nntc_b200_status
     NNTC_B200_ERR_OOM = 3,     /* device memory ran out (src/init.cu:135-149 says it in the user's terms) */
     NNTC_B200_ERR_NODEV = 4,   /* no usable device */
     NNTC_B200_ERR_STATE = 5,   /* the call needs state the handle does not have (e.g. level 0's grid outside bc8) */
-    NNTC_B200_ERR_TIMEOUT = 6  /* a bounded device-side wait gave up; the device status word says where */
+    NNTC_B200_ERR_TIMEOUT = 6, /* a bounded device-side wait gave up; the device status word says where */
+    NNTC_B200_ERR_IO = 7       /* a file could not be written (the asset writer) */
 };
 
 /* The model: src/model.h:56-114 as a fixed-size POD. Fields that are std::vector in the reference carry a count. */
@@ -321,6 +322,20 @@ enum nntc_b200_kernel
 int nntc_b200_kernel_timing(nntc_b200_device* d, int on);
 /* The launches of `kernel` since the last reset and their summed event time; reset != 0 clears every kernel's. */
 int nntc_b200_kernel_stats(nntc_b200_device* d, int kernel, long long* launches, double* ms, int reset);
+
+/* ---- the asset on disk (src/export.cpp:89-146 dds_write, 470-812 write_asset; the layout of docs/FORMAT.md) ----
+ * Writes PREFIX_lat0.dds (PREFIX_lat0a.dds and PREFIX_lat0b.dds for a block-compressed level 0 of three or four
+ * channels), PREFIX_lat1.dds and the JSON descriptor at json_path (PREFIX_nntc.json when null), all from host memory.
+ * Per plane i of the chain, the base first: k1[i] holds level 1's indices (w1 h1 c1 bytes); for a block-compressed level
+ * 0 (m->bc0) ep[i] and sel[i] hold the blocks the refinement chose (blocks c0 2 and blocks c0 16 bytes, the layout
+ * nntc_b200_bc_state_save returns) and are written as they stand, or, when null, k0[i] (w0 h0 c0 bytes) is packed by the
+ * seed pack; an uncompressed level 0 writes k0[i]. m supplies the extents, bits, grids and decoder. source_width and
+ * source_height are the extent before any padding. sizes (three entries, or null) receives the bytes written for level
+ * 0's file(s), level 1's file and the descriptor. Refuses (NNTC_B200_ERR_ARG, nothing written) a non-finite decoder or
+ * grid and a level-1 index that does not read back as itself on its published grid; NNTC_B200_ERR_IO on a failed write. */
+int nntc_b200_write_asset(const nntc_b200_model* m, const uint8_t* const* k0, const uint8_t* const* k1,
+                          const uint8_t* const* ep, const uint8_t* const* sel, int source_width, int source_height,
+                          const char* prefix, const char* json_path, size_t* sizes);
 
 /* ---- probes: what the reference's per-kernel harness reads (src/backend_check_probe.h:20-37) ---- */
 int nntc_b200_probe_normal_equations(nntc_b200_device* d, double* out, size_t n);

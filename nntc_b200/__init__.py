@@ -77,6 +77,7 @@ PROTOTYPES = {
     "nntc_b200_bc_state_save": (_I, [_P, _M, _PPU8, _PPU8]),
     "nntc_b200_bc_state_restore": (_I, [_P, _M, _PPU8, _PPU8]),
     "nntc_b200_bc_pack_blocks": (_I, [_M, _I, _PU8, _PU8, _PU8, _PPU8, _PD, C.POINTER(_S)]),
+    "nntc_b200_write_asset": (_I, [_M, _PPU8, _PPU8, _PPU8, _PPU8, _I, _I, C.c_char_p, C.c_char_p, C.POINTER(_S)]),
     "nntc_b200_encode_defaults": (None, [C.POINTER(abi.EncodeArgs)]),
     "nntc_b200_encode_on_device": (_I, [_P, _M, C.POINTER(abi.EncodeArgs), _PD, C.POINTER(abi.EncodeResult),
                                         _PPU8, _PPU8, _PPU8, _PPU8]),

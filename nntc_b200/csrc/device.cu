@@ -434,6 +434,12 @@ int validate(const nntc_b200_model* m)
 
 }   // namespace
 
+// The model's layout checks, for host code outside this file (the asset writer).
+int nb::validate_model(const nntc_b200_model* m)
+{
+    return validate(m);
+}
+
 extern "C"
 {
 

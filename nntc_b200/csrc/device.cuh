@@ -255,5 +255,7 @@ int upload_grids(nntc_b200_device* d, const nntc_b200_model* m);
 // The monomial matrices of block (b) (level0 = 0) or block (c') (level0 = 1), built on the host from the decoder
 // (src/solve_level1.cu:164-244).
 void build_monomials(const nntc_b200_model& m, int level0, std::vector<double>& p);
+// The layout checks device_create applies to a model (counts, caps, plane sizes); NNTC_B200_OK or ERR_ARG with a message.
+int validate_model(const nntc_b200_model* m);
 
 }   // namespace nb

@@ -1,0 +1,158 @@
+"""The asset writer (nntc_b200_write_asset) against the reference's own assets.
+
+tests/golden/assets holds assets the reference encoder wrote (tests/golden/make_golden_asset.py), one per layout the
+format distinguishes: a block-compressed level 0 of one to four channels (BC4, BC5, BC5 + BC4, BC5 + BC5), a padded
+source, a palette-mode level 0 stored uncompressed and one packed by the seed pack, a single stored level. Each is read
+back (nntc_b200/asset.py), its state handed to the writer, and the writer's output compared with the reference's:
+
+- every .dds file byte for byte (header, level order, block and texel bytes);
+- every descriptor key a reader needs, with the same value (floats as float32, exactly); the prose keys are the
+  writer's own and are not compared.
+
+Where the reference's own reader of the format (tools/dds_decode.py) is present it reads the re-written asset too and
+must report what it reports for the reference's."""
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from nntc_b200 import NntcError, lib, materials
+from nntc_b200 import asset as A
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "assets")
+CASES = json.load(open(os.path.join(GOLDEN, "cases.json")))
+REF_READER = "/root/reference/tools/dds_decode.py"
+
+
+def indices_from_blocks(m, ep, sel):
+    """Level 0's indices from lossless blocks (palette mode at 1-3 bits, where the decoded byte is k 255 / levels)."""
+    k0 = []
+    for i in range(m.nplanes):
+        w, h = m.w0[i], m.h0[i]
+        bx = (w + 3) // 4
+        e = ep[i].reshape(-1, m.c0, 2).astype(np.int32)
+        s = sel[i].reshape(-1, m.c0, 16)
+        k = np.zeros((h, w, m.c0), np.uint8)
+        for c in range(m.c0):
+            levels = (1 << m.bits0[c]) - 1
+            for y in range(h):
+                for x in range(w):
+                    b = (y // 4) * bx + x // 4
+                    r0, r1, j = e[b, c, 0], e[b, c, 1], s[b, c, (y % 4) * 4 + x % 4]
+                    if r0 > r1:
+                        pal = [r0, r1] + [((8 - t) * r0 + (t - 1) * r1) / 7.0 for t in range(2, 8)]
+                    else:
+                        pal = [r0, r1] + [((6 - t) * r0 + (t - 1) * r1) / 5.0 for t in range(2, 6)] + [0, 255]
+                    k[y, x, c] = int(round(pal[j] * levels / 255.0))
+        k0.append(k.ravel())
+    return k0
+
+
+def rewrite(case, out_dir):
+    src = os.path.join(GOLDEN, case)
+    jname = [f for f in os.listdir(src) if f.endswith("_nntc.json")][0]
+    a = A.read_asset(os.path.join(src, jname))
+    m, k1, k0, ep, sel = A.model_from_asset(a)
+    if m.bc0 and not m.l0_bc8:
+        # palette mode packs k0 itself: hand the writer the indices, not the blocks
+        k0, ep, sel = indices_from_blocks(m, ep, sel), None, None
+    js = a.descriptor
+    prefix = os.path.join(out_dir, jname[: -len("_nntc.json")])
+    sizes = A.write_asset(m, prefix, k1, k0=k0, ep=ep, sel=sel,
+                          source_size=(js["source"]["width"], js["source"]["height"]))
+    return src, jname, prefix, sizes
+
+
+def required(js):
+    """The descriptor's keys a reader needs (the format specification's required ones), prose left out."""
+    out = {k: js[k] for k in ("format", "decode", "block", "lod_bias_level1")}
+    out["source"] = {k: v for k, v in js["source"].items() if k != "inputs"}
+    tex = []
+    for t in js["textures"]:
+        e = {k: t[k] for k in ("level", "width", "height", "dxgi_format", "dxgi_format_id", "channels_used",
+                               "channels_stored", "bits_per_channel", "mip_count", "mip_sizes")}
+        e["file"] = t.get("file")
+        e["files"] = t.get("files")
+        e["bc_palette"] = t.get("bc_palette")
+        d = dict(t["dequantise"])
+        d.pop("note")
+        e["dequantise"] = d
+        tex.append(e)
+    out["textures"] = tex
+    dec = {k: js["decoder"][k] for k in ("type", "terms", "C0", "C1", "nin", "nout", "hidden", "output",
+                                        "activation", "leak")}
+    dec["layers"] = js["decoder"]["layers"]
+    out["decoder"] = dec
+    return out
+
+
+def as_f32(x):
+    if isinstance(x, float):
+        return float(np.float32(x))
+    if isinstance(x, list):
+        return [as_f32(v) for v in x]
+    if isinstance(x, dict):
+        return {k: as_f32(v) for k, v in x.items()}
+    return x
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_rewritten_asset_is_the_references(tmp_path, case):
+    src, jname, prefix, sizes = rewrite(case, str(tmp_path))
+    for f in sorted(os.listdir(src)):
+        if f.endswith(".dds"):
+            ours = open(os.path.join(str(tmp_path), f), "rb").read()
+            theirs = open(os.path.join(src, f), "rb").read()
+            assert ours == theirs, (case, f, len(ours), len(theirs))
+    ours = json.load(open(prefix + "_nntc.json"))
+    theirs = json.load(open(os.path.join(src, jname)))
+    assert as_f32(required(ours)) == as_f32(required(theirs)), case
+    dds = sum(os.path.getsize(os.path.join(str(tmp_path), f)) for f in os.listdir(str(tmp_path)) if f.endswith(".dds"))
+    assert sizes[0] + sizes[1] == dds and sizes[2] == os.path.getsize(prefix + "_nntc.json")
+
+
+def test_writer_refuses_what_the_reference_refuses(tmp_path):
+    src = os.path.join(GOLDEN, "bc8_c2_padded")
+    a = A.read_asset(os.path.join(src, "tex0_nntc.json"))
+    m, k1, k0, ep, sel = A.model_from_asset(a)
+    bad = tmp_path / "bad"
+    bad.mkdir()
+    # a decoder weight that is not finite: nothing is written
+    m.dec_w[3] = float("nan")
+    with pytest.raises(NntcError):
+        A.write_asset(m, str(bad / "x"), k1, ep=ep, sel=sel, source_size=(22, 14))
+    assert os.listdir(str(bad)) == []
+    m.dec_w[3] = 0.5
+    # a level-1 grid on which a stored index no longer reads back as itself
+    m.lo1[0] = m.hi1[0]
+    with pytest.raises(NntcError):
+        A.write_asset(m, str(bad / "x"), k1, ep=ep, sel=sel, source_size=(22, 14))
+    assert "read back" in lib().nntc_b200_last_error().decode()
+
+
+@pytest.mark.skipif(not os.path.exists(REF_READER), reason="the reference's reader of the format is not present")
+@pytest.mark.parametrize("case", ["bc8_c3_t2", "palette_plain", "palette_bc"])
+def test_reference_reader_takes_the_rewritten_asset(tmp_path, case):
+    spec = CASES[case]
+    mat = materials.small(spec["seed"], spec["w"], spec["h"], textures=spec["textures"])
+    pngs = materials.save_material(mat, str(tmp_path / "in"))
+    ref_dir = tmp_path / "ref"
+    shutil.copytree(os.path.join(GOLDEN, case), str(ref_dir))
+    ours_dir = tmp_path / "ours"
+    ours_dir.mkdir()
+    _, _, prefix, _ = rewrite(case, str(ours_dir))
+
+    def reader(pre, *args):
+        p = subprocess.run([sys.executable, REF_READER, pre, *args], capture_output=True, text=True, timeout=300)
+        return p.returncode, p.stdout
+
+    for args in (["--grid"], ["--psnr", *pngs]):
+        rc_ours, out_ours = reader(prefix, *args)
+        rc_ref, out_ref = reader(str(ref_dir / "tex0"), *args)
+        assert rc_ours == 0 and rc_ref == 0, (out_ours, out_ref)
+        strip = lambda s: [l for l in s.splitlines() if "tex0" not in l]  # noqa: E731  (lines naming the path differ)
+        assert strip(out_ours) == strip(out_ref), (out_ours, out_ref)
