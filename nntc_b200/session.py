@@ -160,11 +160,30 @@ class Session:
                                               P(pc, C.c_float), P(x, C.c_double), P(prev, C.c_float)), "workspace")
         return dict(stencil=st, grad=g, precond=pc, x=x, prev=prev)
 
-    def encode(self, args: abi.EncodeArgs | None = None):
+    def encode(self, args: abi.EncodeArgs | None = None, outputs: bool = False):
+        """The whole encode (nntc_b200_encode_on_device). With outputs, also returns the shipped state per plane: level
+        0's and level 1's indices and, under bc8, the refined endpoints and selectors - what write_asset takes."""
         if args is None:
             args = abi.EncodeArgs()
             lib().nntc_b200_encode_defaults(C.byref(args))
         r = abi.EncodeResult()
+        out = None
+        ptrs = (None, None, None, None)
+        if outputs:
+            m, n = self.m, self.m.nplanes
+            blocks = [((m.w0[i] + 3) // 4) * ((m.h0[i] + 3) // 4) for i in range(n)]
+            out = dict(k0=[np.zeros(self.n0(i) * m.c0, np.uint8) for i in range(n)],
+                       k1=[np.zeros(self.n1(i) * m.c1, np.uint8) for i in range(n)],
+                       ep=[np.zeros(b * m.c0 * 2, np.uint8) for b in blocks] if m.l0_bc8 else None,
+                       sel=[np.zeros(b * m.c0 * 16, np.uint8) for b in blocks] if m.l0_bc8 else None)
+            ptrs = tuple(abi.u8_ptrs(out[k]) if out[k] is not None else None for k in ("k0", "k1", "ep", "sel"))
         check(lib().nntc_b200_encode_on_device(self.d, C.byref(self.m), C.byref(args), self.per_site, C.byref(r),
-                                               None, None, None, None), "encode")
-        return r
+                                               *ptrs), "encode")
+        return (r, out) if outputs else r
+
+    def write_asset(self, prefix: str, outputs: dict, source_size=None, json_path: str | None = None):
+        """The encode's result as the reference's asset on disk (nntc_b200_write_asset): PREFIX_lat0*.dds,
+        PREFIX_lat1.dds and PREFIX_nntc.json. outputs: what encode(outputs=True) returned."""
+        from . import asset
+        return asset.write_asset(self.m, prefix, outputs["k1"], k0=outputs["k0"], ep=outputs["ep"],
+                                 sel=outputs["sel"], source_size=source_size, json_path=json_path)
