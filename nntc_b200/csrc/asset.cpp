@@ -186,6 +186,12 @@ extern "C" int nntc_b200_write_asset(const nntc_b200_model* m, const uint8_t* co
     for (int c = 0; c < c0; c++)
         if (m->bits0[c] < 1 || m->bits0[c] > 8)
             return arg_error("write_asset: level 0's bits per channel must be 1..8");
+    for (int i = 0; i < np && k0; i++)
+        if (k0[i] && !(compress && ep && sel && ep[i] && sel[i]))
+            for (size_t t = 0; t < (size_t)m->w0[i] * m->h0[i] * c0; t++)
+                if (k0[i][t] > (1 << m->bits0[t % c0]) - 1)
+                    return arg_error("write_asset: a level-0 index of plane " + std::to_string(i) +
+                                     " is above its channel's bits");
     if (m->bits1 < 4 || m->bits1 > 8)
         return arg_error("write_asset: level 1's bits per channel must be 4..8");
 
