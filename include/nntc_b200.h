@@ -329,7 +329,7 @@ int nntc_b200_kernel_stats(nntc_b200_device* d, int kernel, long long* launches,
  * Per plane i of the chain, the base first: k1[i] holds level 1's indices (w1 h1 c1 bytes); for a block-compressed level
  * 0 (m->bc0) ep[i] and sel[i] hold the blocks the refinement chose (blocks c0 2 and blocks c0 16 bytes, the layout
  * nntc_b200_bc_state_save returns) and are written as they stand, or, when null, k0[i] (w0 h0 c0 bytes) is packed by the
- * seed pack; an uncompressed level 0 writes k0[i]. m supplies the extents, bits, grids and decoder. source_width and
+ * seed pack; an uncompressed level 0 writes k0[i] (under bc8 that is the reference's uncompressed twin, --bc0 both). m supplies the extents, bits, grids and decoder. source_width and
  * source_height are the extent before any padding. sizes (three entries, or null) receives the bytes written for level
  * 0's file(s), level 1's file and the descriptor. Refuses (NNTC_B200_ERR_ARG, nothing written) a non-finite decoder or
  * grid and a level-1 index that does not read back as itself on its published grid; NNTC_B200_ERR_IO on a failed write. */

@@ -165,8 +165,6 @@ extern "C" int nntc_b200_write_asset(const nntc_b200_model* m, const uint8_t* co
     NB_TRY(validate_model(m));
     const int np = m->nplanes, c0 = m->c0, c1 = m->c1, nout = m->nout, nin = m->nin;
     const bool compress = m->bc0 != 0;
-    if (m->l0_bc8 && !compress)
-        return arg_error("write_asset: --l0 bc8 ships level 0 block-compressed (bc0 must be set)");
     if (!m->has_decoder)
         return arg_error("write_asset: the model has no decoder to publish");
     // A non-finite number would be written as a token no JSON parser reads: refuse the asset instead.

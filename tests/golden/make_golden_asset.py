@@ -33,6 +33,7 @@ CASES = {
                                                                  "--c1", "1"]),
     "palette_bc": dict(seed=16, w=36, h=28, textures=1, args=["--l0", "palette", "--bits0", "3", "--c0", "3"]),
     "one_level": dict(seed=17, w=24, h=24, textures=1, args=["--mips", "0"]),
+    "bc8_twin": dict(seed=18, w=24, h=20, textures=1, args=["--bc0", "both"]),
 }
 
 

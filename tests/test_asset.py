@@ -52,9 +52,13 @@ def indices_from_blocks(m, ep, sel):
     return k0
 
 
-def rewrite(case, out_dir):
+def descriptors(case):
+    return sorted(f for f in os.listdir(os.path.join(GOLDEN, case)) if f.endswith("_nntc.json"))
+
+
+def rewrite(case, out_dir, jname=None):
     src = os.path.join(GOLDEN, case)
-    jname = [f for f in os.listdir(src) if f.endswith("_nntc.json")][0]
+    jname = jname or descriptors(case)[0]
     a = A.read_asset(os.path.join(src, jname))
     m, k1, k0, ep, sel = A.model_from_asset(a)
     if m.bc0 and not m.l0_bc8:
@@ -100,18 +104,21 @@ def as_f32(x):
     return x
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
-def test_rewritten_asset_is_the_references(tmp_path, case):
-    src, jname, prefix, sizes = rewrite(case, str(tmp_path))
-    for f in sorted(os.listdir(src)):
-        if f.endswith(".dds"):
-            ours = open(os.path.join(str(tmp_path), f), "rb").read()
-            theirs = open(os.path.join(src, f), "rb").read()
-            assert ours == theirs, (case, f, len(ours), len(theirs))
+@pytest.mark.parametrize("case,jname", [(c, j) for c in sorted(CASES) for j in descriptors(c)])
+def test_rewritten_asset_is_the_references(tmp_path, case, jname):
+    src, jname, prefix, sizes = rewrite(case, str(tmp_path), jname)
+    stem = jname[: -len("_nntc.json")]
+    ours_dds = sorted(f for f in os.listdir(str(tmp_path)) if f.endswith(".dds"))
+    theirs_dds = sorted(f for f in os.listdir(src) if f.endswith(".dds") and f[len(stem):].startswith("_lat"))
+    assert ours_dds == theirs_dds, (case, ours_dds, theirs_dds)
+    for f in ours_dds:
+        ours = open(os.path.join(str(tmp_path), f), "rb").read()
+        theirs = open(os.path.join(src, f), "rb").read()
+        assert ours == theirs, (case, f, len(ours), len(theirs))
     ours = json.load(open(prefix + "_nntc.json"))
     theirs = json.load(open(os.path.join(src, jname)))
     assert as_f32(required(ours)) == as_f32(required(theirs)), case
-    dds = sum(os.path.getsize(os.path.join(str(tmp_path), f)) for f in os.listdir(str(tmp_path)) if f.endswith(".dds"))
+    dds = sum(os.path.getsize(os.path.join(str(tmp_path), f)) for f in ours_dds)
     assert sizes[0] + sizes[1] == dds and sizes[2] == os.path.getsize(prefix + "_nntc.json")
 
 
