@@ -179,3 +179,82 @@ def model_from_asset(a: Asset):
             shift = np.array([8 - m.bits0[c] for c in range(m.c0)], np.int32)
             k0.append((b >> shift).astype(np.uint8).ravel())
     return m, k1, k0, ep, sel
+
+
+def _bc4_plane(blocks: bytes, w: int, h: int, stride: int, offset: int) -> np.ndarray:
+    """One channel of a BC4/BC5 level as the float bytes the standard palette decodes to (h x w)."""
+    bx, by = (w + 3) // 4, (h + 3) // 4
+    ep, sel = bc4_fields(blocks, bx * by, stride, offset)
+    r0, r1 = ep[:, 0].astype(np.float64), ep[:, 1].astype(np.float64)
+    pal = np.empty((bx * by, 8))
+    pal[:, 0], pal[:, 1] = r0, r1
+    wide = r0 > r1
+    for i in range(2, 8):
+        six = ((6 - i) * r0 + (i - 1) * r1) / 5.0 if i < 6 else np.full_like(r0, 0.0 if i == 6 else 255.0)
+        pal[:, i] = np.where(wide, ((8 - i) * r0 + (i - 1) * r1) / 7.0, six)
+    texel = np.take_along_axis(pal, sel.astype(np.intp), axis=1)            # (blocks, 16), row-major in the block
+    img = texel.reshape(by, bx, 4, 4).transpose(0, 2, 1, 3).reshape(by * 4, bx * 4)
+    return img[:h, :w]
+
+
+def sampled_bytes(a: Asset, level: int, mip: int) -> np.ndarray:
+    """What a UNORM sampler holds for one texture at one mip, in bytes (h x w x channels_used, float)."""
+    tex = a.descriptor["textures"][level]
+    w, h = tex["mip_sizes"][mip]
+    used = tex["channels_used"]
+    if level == 0 and a.level0[0].compressed:
+        planes = []
+        for f in a.level0:
+            nc = 1 if f.dxgi == 80 else 2
+            planes += [_bc4_plane(f.levels[mip], w, h, f.block_bytes, 8 * c) for c in range(nc)]
+        return np.stack(planes, axis=-1)[:, :, :used]
+    f = a.level0[0] if level == 0 else a.level1
+    return np.frombuffer(f.levels[mip], np.uint8).reshape(h, w, f.block_bytes)[:, :, :used].astype(np.float64)
+
+
+def decode(a: Asset, mip: int = 0) -> np.ndarray:
+    """The material one mip of the asset decodes to, at level 0's texel centres: level 0 read at the texel, level 1
+    sampled bilinearly with clamped taps, both dequantised after sampling (lo + byte / 255 (hi - lo)), phi in the
+    descriptor's term order, out = W phi + b, saturated and rounded half up to 8 bits. h x w x 3T bytes."""
+    js = a.descriptor
+    t0, t1 = js["textures"]
+    dec = js["decoder"]
+    if dec["type"] != "bilinear" or dec["terms"].split() != ["a", "b", "sc"] or dec["hidden"]:
+        raise ValueError("a decoder this format does not describe")
+
+    def value(level, tex):
+        dq = tex["dequantise"]
+        lo = np.asarray(dq["lo"], np.float64)[None, None, :]
+        hi = np.asarray(dq["hi"], np.float64)[None, None, :]
+        return lo + sampled_bytes(a, level, mip) / 255.0 * (hi - lo)
+
+    s = value(0, t0)
+    z1 = value(1, t1)
+    h, w = s.shape[:2]
+    h1, w1 = z1.shape[:2]
+    x = (np.arange(w) + 0.5) / w * w1 - 0.5
+    y = (np.arange(h) + 0.5) / h * h1 - 0.5
+    xf, yf = np.floor(x), np.floor(y)
+    fx, fy = (x - xf)[None, :, None], (y - yf)[:, None, None]
+    xa, xb = np.clip(xf.astype(int), 0, w1 - 1), np.clip(xf.astype(int) + 1, 0, w1 - 1)
+    ya, yb = np.clip(yf.astype(int), 0, h1 - 1), np.clip(yf.astype(int) + 1, 0, h1 - 1)
+    c = (z1[ya][:, xa] * (1 - fx) + z1[ya][:, xb] * fx) * (1 - fy) + (z1[yb][:, xa] * (1 - fx) + z1[yb][:, xb] * fx) * fy
+    c0, c1 = dec["C0"], dec["C1"]
+    phi = np.concatenate([c, s, (s[:, :, :, None] * c[:, :, None, :]).reshape(h, w, c0 * c1)], axis=-1)
+    layer = dec["layers"][0]
+    W = np.asarray(layer["weights"], np.float64).reshape(layer["rows"], layer["cols"])
+    out = phi @ W.T + np.asarray(layer["bias"], np.float64)
+    return np.floor(np.clip(out, 0.0, 1.0) * 255.0 + 0.5).astype(np.uint8)
+
+
+def psnr(a: Asset, sources) -> list:
+    """Per texture, the PSNR of the decoded base level against its source image (h x w x 3 bytes) over the source's
+    extent (the asset may be padded)."""
+    img = decode(a, 0).astype(np.float64)
+    out = []
+    for t, src in enumerate(sources):
+        src = np.asarray(src, np.float64)
+        h, w = src.shape[:2]
+        mse = float(np.mean((img[:h, :w, 3 * t:3 * t + 3] - src) ** 2))
+        out.append(10.0 * np.log10(255.0 * 255.0 / mse) if mse > 0 else 100.0)
+    return out

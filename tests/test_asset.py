@@ -13,12 +13,14 @@ Where the reference's own reader of the format (tools/dds_decode.py) is present 
 must report what it reports for the reference's."""
 import json
 import os
+import re
 import shutil
 import subprocess
 import sys
 
 import numpy as np
 import pytest
+from PIL import Image
 
 from nntc_b200 import NntcError, lib, materials
 from nntc_b200 import asset as A
@@ -163,3 +165,9 @@ def test_reference_reader_takes_the_rewritten_asset(tmp_path, case):
         assert rc_ours == 0 and rc_ref == 0, (out_ours, out_ref)
         strip = lambda s: [l for l in s.splitlines() if "tex0" not in l]  # noqa: E731  (lines naming the path differ)
         assert strip(out_ours) == strip(out_ref), (out_ours, out_ref)
+    # this package's own decoder of the format agrees with the reference's reader (which prints two decimals)
+    quoted = [float(re.search(r"psnr ([0-9.]+) dB", l).group(1)) for l in out_ref.splitlines()
+              if re.match(r"\s*texture \d+:", l)]
+    sources = [np.asarray(Image.open(p).convert("RGB")) for p in pngs]
+    ours = A.psnr(A.read_asset(prefix + "_nntc.json"), sources)
+    assert len(quoted) == len(ours) and all(abs(a - b) <= 0.0051 for a, b in zip(ours, quoted)), (ours, quoted)
