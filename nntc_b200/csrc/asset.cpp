@@ -213,6 +213,14 @@ extern "C" int nntc_b200_write_asset(const nntc_b200_model* m, const uint8_t* co
         int bits[NNTC_B200_MAX_CHANNELS];
         for (int c = 0; c < c1; c++)
             bits[c] = m->bits1;
+        // whether index k of channel c reads back as itself: a property of (c, k) alone, so it is settled once per
+        // value and looked up per texel
+        bool reads_back[NNTC_B200_MAX_CHANNELS][256];
+        for (int c = 0; c < c1; c++)
+            for (int k = 0; k < 256; k++)
+                reads_back[c][k] =
+                    k <= (1 << m->bits1) - 1 &&
+                    grid_index(m->lo1[c], m->hi1[c], m->bits1, grid_value(m->lo1[c], m->hi1[c], m->bits1, k)) == k;
         std::vector<std::vector<uint8_t>> levels((size_t)np);
         for (int i = 0; i < np; i++)
         {
@@ -220,8 +228,7 @@ extern "C" int nntc_b200_write_asset(const nntc_b200_model* m, const uint8_t* co
             for (size_t t = 0; t < texels * c1; t++)
             {
                 const int c = (int)(t % c1), k = k1[i][t];
-                if (k > (1 << m->bits1) - 1 ||
-                    grid_index(m->lo1[c], m->hi1[c], m->bits1, grid_value(m->lo1[c], m->hi1[c], m->bits1, k)) != k)
+                if (!reads_back[c][k])
                     return arg_error("write_asset: level-1 index " + std::to_string(k) + " of channel " +
                                      std::to_string(c) + " does not read back as itself on its published grid");
             }
