@@ -72,8 +72,16 @@ def read_dds(path: str, sizes) -> DdsFile:
     if hd[0] != 0x20534444 or hd[1] != 124 or hd[21] != 0x30315844:
         raise ValueError(f"{path}: not a DX10 .dds")
     f = DdsFile(width=hd[4], height=hd[3], dxgi=hd[32], flags=hd[2], size_field=hd[5], caps=hd[27])
-    if hd[7] != len(sizes):
-        raise ValueError(f"{path}: {hd[7]} levels stored, the descriptor lists {len(sizes)}")
+    if f.dxgi not in DXGI or hd[33] != 3 or hd[35] != 1:
+        raise ValueError(f"{path}: not a 2D texture of a format the asset uses")
+    if hd[7] != len(sizes) or [f.width, f.height] != list(sizes[0]):
+        raise ValueError(f"{path}: {hd[7]} levels of {f.width}x{f.height}, the descriptor lists {sizes}")
+    chain = len(sizes) > 1
+    want_flags = 0x1007 | (0x20000 if chain else 0) | (0x80000 if f.compressed else 0x8)
+    want_size = (((f.width + 3) // 4) * ((f.height + 3) // 4) * f.block_bytes if f.compressed
+                 else f.width * f.block_bytes)
+    if f.flags != want_flags or f.caps != (0x401008 if chain else 0x1000) or f.size_field != want_size:
+        raise ValueError(f"{path}: header flags, caps or size field do not describe the stored levels")
     at = 148
     for w, h in sizes:
         n = ((w + 3) // 4) * ((h + 3) // 4) * f.block_bytes if f.compressed else w * h * f.block_bytes
