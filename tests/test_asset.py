@@ -171,3 +171,26 @@ def test_reference_reader_takes_the_rewritten_asset(tmp_path, case):
     sources = [np.asarray(Image.open(p).convert("RGB")) for p in pngs]
     ours = A.psnr(A.read_asset(prefix + "_nntc.json"), sources)
     assert len(quoted) == len(ours) and all(abs(a - b) <= 0.0051 for a, b in zip(ours, quoted)), (ours, quoted)
+
+
+REF_EXAMPLES = "/root/reference/examples"
+SHIPPED = ["m1_m4_c0_3_c1_4", "pavingstones141_1k_c0_4"]
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="the reference's example assets are not present")
+@pytest.mark.parametrize("stem", SHIPPED)
+def test_rewritten_shipped_example_is_the_references(tmp_path, stem):
+    """The example assets the reference ships (a 512 x 512 four-texture material at C0 = 3 and a 1K five-texture one at
+    C0 = 4), re-written from their own state: the same .dds bytes and the same descriptor keys."""
+    jpath = os.path.join(REF_EXAMPLES, stem + "_nntc.json")
+    if not os.path.exists(jpath):
+        pytest.skip(f"{stem} is not among the reference's examples")
+    a = A.read_asset(jpath)
+    m, k1, k0, ep, sel = A.model_from_asset(a)
+    js = a.descriptor
+    prefix = str(tmp_path / stem)
+    A.write_asset(m, prefix, k1, k0=k0, ep=ep, sel=sel, source_size=(js["source"]["width"], js["source"]["height"]))
+    for f in sorted(os.listdir(str(tmp_path))):
+        if f.endswith(".dds"):
+            assert open(os.path.join(str(tmp_path), f), "rb").read() == open(os.path.join(REF_EXAMPLES, f), "rb").read(), f
+    assert as_f32(required(json.load(open(prefix + "_nntc.json")))) == as_f32(required(js))
