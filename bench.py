@@ -355,7 +355,7 @@ def roofline(name, stat, mat, hbm, tf, src):
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": src,
             "traffic_source": "ncu DRAM bytes of the 4x2048x1024 workload scaled by level-0 pixels" if traffic
-            else "no ncu capture of this build's kernels of this group",
+            else "no ncu DRAM figure recorded for this group's current kernels",
             "binding": BINDING.get(name), "bytes_per_launch": per, "launches": launches,
             "ms_per_launch": round(ms / launches, 4)}
 
