@@ -11,6 +11,7 @@ back (nntc_b200/asset.py), its state handed to the writer, and the writer's outp
 
 Where the reference's own reader of the format (tools/dds_decode.py) is present it reads the re-written asset too and
 must report what it reports for the reference's."""
+import ctypes as C
 import json
 import os
 import re
@@ -22,7 +23,7 @@ import numpy as np
 import pytest
 from PIL import Image
 
-from nntc_b200 import NntcError, lib, materials
+from nntc_b200 import NntcError, abi, check, lib, materials
 from nntc_b200 import asset as A
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "assets")
@@ -194,3 +195,28 @@ def test_rewritten_shipped_example_is_the_references(tmp_path, stem):
         if f.endswith(".dds"):
             assert open(os.path.join(str(tmp_path), f), "rb").read() == open(os.path.join(REF_EXAMPLES, f), "rb").read(), f
     assert as_f32(required(json.load(open(prefix + "_nntc.json")))) == as_f32(required(js))
+
+
+@pytest.mark.parametrize("case", ["bc8_c1", "bc8_c3_t2", "bc8_c4_t4", "palette_bc"])
+def test_bc_pack_blocks_gives_the_files_blocks(case):
+    """nntc_b200_bc_pack_blocks (the seam's host pack, src/export.cpp:333-370) turns each plane's endpoints and
+    selectors into the reference's file bytes; on a lossless palette-mode plane its error against k0 is the float
+    rounding of the palette (the decoded entry is a float division by 7, the exact value a double one)."""
+    src = os.path.join(GOLDEN, case)
+    a = A.read_asset(os.path.join(src, descriptors(case)[0]))
+    m, k1, k0, ep, sel = A.model_from_asset(a)
+    lossless = not m.l0_bc8
+    if lossless:
+        k0 = indices_from_blocks(m, ep, sel)
+    for i in range(m.nplanes):
+        files = [np.zeros(len(f.levels[i]), np.uint8) for f in a.level0]
+        se, n = C.c_double(0.0), C.c_size_t(0)
+        kk = np.ascontiguousarray(k0[i]) if lossless else None
+        check(lib().nntc_b200_bc_pack_blocks(C.byref(m), i, ep[i].ctypes.data_as(C.POINTER(C.c_uint8)),
+                                             sel[i].ctypes.data_as(C.POINTER(C.c_uint8)),
+                                             kk.ctypes.data_as(C.POINTER(C.c_uint8)) if kk is not None else None,
+                                             abi.u8_ptrs(files), C.byref(se), C.byref(n)), "bc_pack_blocks")
+        for f, mine in zip(a.level0, files):
+            assert mine.tobytes() == f.levels[i], (case, i)
+        if lossless:
+            assert se.value <= 1e-9 * n.value and n.value == m.w0[i] * m.h0[i] * m.c0
