@@ -1,8 +1,9 @@
 // decoder.cu: block (a), the decoder as one global least squares (src/solve_decoder.cu:1-458).
 //
 // With v = [phi ; 1] (mm = nin + 1) and the target t, the normal equations are A = sum omega v v^T (upper triangle)
-// and rhs_c = sum omega v t_c; W and b follow by Gauss-Jordan with the ridge ladder {1e-9, 1e-12, 0} mean(diag A)
-// and the acceptance test on the objective's own quadratic Q (src/solve_decoder.cu:184-458), on the host.
+// and rhs_c = sum omega v t_c; W and b follow from an FP64 Cholesky solve on the device with one refinement step,
+// under the ridge ladder {1e-9, 1e-12, 0} mean(diag A) and the acceptance test on the objective's own quadratic Q
+// (the semantics of src/solve_decoder.cu:184-458; the solver is this file's own, see k_decoder_solve).
 //
 // The accumulation, B200 shape: every product is a float times a float, exact in double, and the entries needed are
 // blocks of the Gram of Z = [phi | 1 | t] over all sites, so they run on the FP64 tensor cores (k_ls_accumulate_mma
@@ -236,166 +237,292 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     return block_end(d, ms);
 }
 
-// ---- the host solve (src/solve_decoder.cu:184-458) -----------------------------------------------------------------
+// ---- the solve, on the device ---------------------------------------------------------------------------------------
+//
+// The system is tiny (mm <= 25 unknowns, nout <= 18 right-hand sides), so one block of 128 threads does all of it in
+// shared memory, with no host round trip between the accumulation and the decision:
+//
+//   for each ridge r of the ladder {1e-9, 1e-12, 0} x mean(diag A), until one is accepted:
+//     L L^T = A + r I                       FP64 Cholesky, right-looking, a non-positive or non-finite pivot refuses
+//                                           the rung;
+//     X = (L L^T)^-1 R                      one forward and one backward substitution per output;
+//     X += (L L^T)^-1 (R - (A + r I) X)     one step of iterative refinement, the residual with fused multiply-adds;
+//     X rounded to float                    the decoder that would ship; a non-finite value refuses the rung;
+//     accept X if Q(X) does not exceed Q(previous decoder) by more than 1e-12 in E's units once both quadratics'
+//     rounding bounds are charged against the difference (or if there is no previous decoder).
+//
+// Q(x) = sum_c cw_c (x_c^T A x_c - 2 x_c . R_c) is E's numerator up to a constant, so the test costs no objective pass;
+// its rounding bound is eps mm sum_c cw_c (|x_c|^T |A| |x_c| + 2 |x_c| . |R_c|). These semantics - the rungs, the float
+// rounding before judging, the bound and the 1e-12 tolerance, keeping the previous decoder when every rung is refused
+// and the weighted mean target when there is none - are the reference's (src/solve_decoder.cu:267-458); the solver is
+// not (the reference runs Gauss-Jordan with partial pivoting on the host). A Cholesky pivot that is not positive
+// refuses a rung where Gauss-Jordan would have pivoted on, which the acceptance test would refuse in any case: such a
+// system's ridge-free solution is not a minimiser of Q.
 
-static bool gauss_jordan(std::vector<double>& g, int m, int nrhs)
+constexpr int DS_THREADS = 128;
+constexpr int DS_MM = MAX_NIN + 1;
+
+struct DecoderSolveArgs
 {
-    const int cols = m + nrhs;
-    for (int k = 0; k < m; k++)
-    {
-        int pivot = k;
-        double best = std::fabs(g[(size_t)k * cols + k]);
-        for (int i = k + 1; i < m; i++)
-        {
-            const double a = std::fabs(g[(size_t)i * cols + k]);
-            if (a > best)
-            {
-                best = a;
-                pivot = i;
-            }
-        }
-        if (best == 0.0)
-            return false;
-        if (pivot != k)
-            for (int j = 0; j < cols; j++)
-                std::swap(g[(size_t)k * cols + j], g[(size_t)pivot * cols + j]);
-        const double inv = 1.0 / g[(size_t)k * cols + k];
-        for (int j = 0; j < cols; j++)
-            g[(size_t)k * cols + j] *= inv;
-        for (int i = 0; i < m; i++)
-        {
-            if (i == k)
-                continue;
-            const double f = g[(size_t)i * cols + k];
-            if (f == 0.0)
-                continue;
-            for (int j = 0; j < cols; j++)
-                g[(size_t)i * cols + j] -= f * g[(size_t)k * cols + j];
-        }
-    }
-    return true;
-}
+    int nin, nout;
+    int had_previous;   // the model arrives with a decoder
+    int norm_ok;        // sum(cw) x the weighted site count > 0
+    double inv_norm;    // 1 / (sum(cw) x the weighted site count): Q in E's units
+    float cw[MAX_NOUT];
+    float w[MAX_NOUT * MAX_NIN];
+    float b[MAX_NOUT];
+};
 
-static const double RIDGE_LADDER[] = { 1e-9, 1e-12, 0.0 };
-static const double LS_ACCEPT_RISE = 1e-12;
-static long long g_ridge_tally[4] = { 0, 0, 0, 0 };
-
-// The decoder from the normal equations in acc (the ladder, the acceptance test and the fallbacks). Returns the rung
-// taken (0..2), or 3 when every rung was refused.
-int decoder_from_normal_equations(nntc_b200_model& m, int k, const double* per_site, const std::vector<double>& acc)
+// What the solve hands back: the rung taken (0..2), 3 with a fallback fit (no previous decoder), 4 when the previous
+// decoder stays; then, unless 4, the decoder as nout rows of [w_c (nin) | b_c].
+struct DecoderSolveOut
 {
-    const int nin = m.nin, nout = m.nout, mm = nin + 1;
-    const int tri = mm * (mm + 1) / 2;
-    double trace = 0.0;
-    for (int i = 0; i < mm; i++)
-        trace += acc[(size_t)tri_index(i, i, mm)];
-    const double mean_diag = trace > 0.0 ? trace / mm : 1.0;
+    int rung;
+    int pad[3];
+    float x[MAX_NOUT * DS_MM];
+};
 
-    const bool had_previous = m.has_decoder != 0;
-    std::vector<double> x_prev((size_t)nout * mm, 0.0);
-    if (had_previous)
-        for (int c = 0; c < nout; c++)
-        {
-            for (int i = 0; i < nin; i++)
-                x_prev[(size_t)c * mm + i] = (double)m.dec_w[(size_t)c * nin + i];
-            x_prev[(size_t)c * mm + nin] = (double)m.dec_b[c];
-        }
-    double sum_cw = 0.0;
-    for (int c = 0; c < nout; c++)
-        sum_cw += (double)m.cw[c];
-    double den = 0.0;
-    for (int i = 0; i < m.nplanes; i++)
-        den += per_site[i] * (double)m.w0[i] * (double)m.h0[i] * (double)(1 + k);
-    const bool norm_ok = sum_cw * den > 0.0;
-    const double inv_norm = norm_ok ? 1.0 / (sum_cw * den) : 0.0;
-
-    auto qform = [&](const std::vector<double>& x, double& err) {
-        double q = 0.0, e = 0.0;
-        for (int c = 0; c < nout; c++)
-        {
-            double qc = 0.0, ec = 0.0;
-            for (int i = 0; i < mm; i++)
-            {
-                for (int j = 0; j < mm; j++)
-                {
-                    const double a = i <= j ? acc[(size_t)tri_index(i, j, mm)] : acc[(size_t)tri_index(j, i, mm)];
-                    qc += x[(size_t)c * mm + i] * a * x[(size_t)c * mm + j];
-                    ec += std::fabs(x[(size_t)c * mm + i]) * std::fabs(a) * std::fabs(x[(size_t)c * mm + j]);
-                }
-                qc -= 2.0 * x[(size_t)c * mm + i] * acc[(size_t)tri + (size_t)c * mm + i];
-                ec += 2.0 * std::fabs(x[(size_t)c * mm + i]) * std::fabs(acc[(size_t)tri + (size_t)c * mm + i]);
-            }
-            q += (double)m.cw[c] * qc;
-            e += (double)m.cw[c] * ec;
-        }
-        err = DBL_EPSILON * (double)mm * e * inv_norm;
-        return q;
-    };
-
-    double err_prev = 0.0;
-    const double q_prev = had_previous ? qform(x_prev, err_prev) : 0.0;
-    const int cols = mm + nout;
-    std::vector<double> g((size_t)mm * cols, 0.0);
-    std::vector<double> x_new((size_t)nout * mm, 0.0);
-    bool accepted = false;
-    int taken = 0;
-    for (int step = 0; step < 3 && !accepted; step++)
+// The quadratic and its rounding bound at the solution rows X (shared), in E's units for the bound. Every thread
+// calls it; thread c < nout forms output c's terms, thread 0 adds the outputs in index order.
+__device__ void ds_quadratic(const double (*A)[DS_MM + 1], const double (*R)[DS_MM], const double (*X)[DS_MM],
+                             const DecoderSolveArgs& a, int mm, double* qc, double* ec, double& q, double& err)
+{
+    const int c = threadIdx.x;
+    if (c < a.nout)
     {
-        const double ridge = RIDGE_LADDER[step] * mean_diag;
-        std::fill(g.begin(), g.end(), 0.0);
+        double qs = 0.0, es = 0.0;
         for (int i = 0; i < mm; i++)
         {
-            for (int j = i; j < mm; j++)
+            double ax = 0.0, aax = 0.0;
+            for (int j = 0; j < mm; j++)
             {
-                const double a = acc[(size_t)tri_index(i, j, mm)];
-                g[(size_t)i * cols + j] = a;
-                g[(size_t)j * cols + i] = a;
+                ax = fma(A[i][j], X[c][j], ax);
+                aax = fma(fabs(A[i][j]), fabs(X[c][j]), aax);
             }
-            g[(size_t)i * cols + i] += ridge;
-            for (int c = 0; c < nout; c++)
-                g[(size_t)i * cols + mm + c] = acc[(size_t)tri + (size_t)c * mm + i];
+            qs = fma(X[c][i], ax - 2.0 * R[c][i], qs);
+            es = fma(fabs(X[c][i]), aax + 2.0 * fabs(R[c][i]), es);
         }
-        if (!gauss_jordan(g, mm, nout))
+        qc[c] = qs;
+        ec[c] = es;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double qt = 0.0, et = 0.0;
+        for (int o = 0; o < a.nout; o++)
+        {
+            qt += (double)a.cw[o] * qc[o];
+            et += (double)a.cw[o] * ec[o];
+        }
+        q = qt;
+        err = DBL_EPSILON * (double)mm * et * a.inv_norm;
+    }
+    __syncthreads();
+}
+
+// Solve (L L^T) y = rhs in place for output row c (one thread).
+__device__ void ds_substitute(const double (*L)[DS_MM + 1], double* y, int mm)
+{
+    for (int i = 0; i < mm; i++)
+    {
+        double s = y[i];
+        for (int j = 0; j < i; j++)
+            s = fma(-L[i][j], y[j], s);
+        y[i] = s / L[i][i];
+    }
+    for (int i = mm - 1; i >= 0; i--)
+    {
+        double s = y[i];
+        for (int j = i + 1; j < mm; j++)
+            s = fma(-L[j][i], y[j], s);
+        y[i] = s / L[i][i];
+    }
+}
+
+__global__ void __launch_bounds__(DS_THREADS) k_decoder_solve(const double* __restrict__ ne, DecoderSolveArgs a,
+                                                               DecoderSolveOut* out)
+{
+    __shared__ double A[DS_MM][DS_MM + 1], L[DS_MM][DS_MM + 1];
+    __shared__ double R[MAX_NOUT][DS_MM], X[MAX_NOUT][DS_MM], D[MAX_NOUT][DS_MM];
+    __shared__ double qc[MAX_NOUT], ec[MAX_NOUT];
+    __shared__ double q_prev, err_prev, q_new, err_new, mean_diag;
+    __shared__ int refused, accepted;
+    const int tid = threadIdx.x, nin = a.nin, nout = a.nout, mm = nin + 1;
+    const int tri = mm * (mm + 1) / 2;
+
+    // A from its upper triangle, R from the right-hand-side rows (output c's rhs is the c-th run of mm entries)
+    for (int e = tid; e < mm * mm; e += DS_THREADS)
+    {
+        const int i = e / mm, j = e % mm, lo = min(i, j), hi = max(i, j);
+        A[i][j] = ne[tri_index(lo, hi, mm)];
+    }
+    for (int e = tid; e < nout * mm; e += DS_THREADS)
+        R[e / mm][e % mm] = ne[tri + e];
+    // the previous decoder as solution rows, for its quadratic
+    for (int e = tid; e < nout * mm; e += DS_THREADS)
+    {
+        const int c = e / mm, i = e % mm;
+        X[c][i] = a.had_previous ? (double)(i < nin ? a.w[c * nin + i] : a.b[c]) : 0.0;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        double trace = 0.0;
+        for (int i = 0; i < mm; i++)
+            trace += A[i][i];
+        mean_diag = trace > 0.0 ? trace / mm : 1.0;
+        accepted = -1;
+    }
+    __syncthreads();
+    if (a.had_previous)
+        ds_quadratic(A, R, X, a, mm, qc, ec, q_prev, err_prev);
+
+    const double ladder[3] = { 1e-9, 1e-12, 0.0 };
+    for (int rung = 0; rung < 3; rung++)
+    {
+        const double ridge = ladder[rung] * mean_diag;
+        for (int e = tid; e < mm * mm; e += DS_THREADS)
+        {
+            const int i = e / mm, j = e % mm;
+            L[i][j] = i == j ? A[i][j] + ridge : A[i][j];
+        }
+        if (tid == 0)
+            refused = 0;
+        __syncthreads();
+        // right-looking Cholesky on the lower triangle
+        for (int k = 0; k < mm; k++)
+        {
+            if (tid == 0)
+            {
+                const double p = L[k][k];
+                if (p > 0.0 && isfinite(p))
+                    L[k][k] = sqrt(p);
+                else
+                    refused = 1;
+            }
+            __syncthreads();
+            if (refused)
+                break;
+            for (int i = k + 1 + tid; i < mm; i += DS_THREADS)
+                L[i][k] /= L[k][k];
+            __syncthreads();
+            const int n = mm - k - 1;
+            for (int e = tid; e < n * n; e += DS_THREADS)
+            {
+                const int i = k + 1 + e / n, j = k + 1 + e % n;
+                if (j <= i)
+                    L[i][j] = fma(-L[i][k], L[j][k], L[i][j]);
+            }
+            __syncthreads();
+        }
+        if (refused)
             continue;
-        bool finite = true;
-        for (int c = 0; c < nout; c++)
+        // solve, then one refinement step against A + ridge I
+        if (tid < nout)
+        {
             for (int i = 0; i < mm; i++)
-            {
-                const double v = (double)(float)g[(size_t)i * cols + mm + c];
-                x_new[(size_t)c * mm + i] = v;
-                finite = finite && std::isfinite(v);
-            }
-        if (!finite)
+                D[tid][i] = R[tid][i];
+            ds_substitute(L, D[tid], mm);
+        }
+        __syncthreads();
+        for (int e = tid; e < nout * mm; e += DS_THREADS)
+            X[e / mm][e % mm] = D[e / mm][e % mm];
+        __syncthreads();
+        for (int e = tid; e < nout * mm; e += DS_THREADS)
+        {
+            const int c = e / mm, i = e % mm;
+            double r = fma(-ridge, X[c][i], R[c][i]);
+            for (int j = 0; j < mm; j++)
+                r = fma(-A[i][j], X[c][j], r);
+            D[c][i] = r;
+        }
+        __syncthreads();
+        if (tid < nout)
+            ds_substitute(L, D[tid], mm);
+        __syncthreads();
+        int finite = 1;
+        for (int e = tid; e < nout * mm; e += DS_THREADS)
+        {
+            const int c = e / mm, i = e % mm;
+            const double v = (double)(float)(X[c][i] + D[c][i]);
+            X[c][i] = v;
+            finite &= isfinite(v) ? 1 : 0;
+        }
+        if (!__syncthreads_and(finite))
             continue;
-        double err_cand = 0.0;
-        const double q_cand = qform(x_new, err_cand);
-        if (!had_previous || (norm_ok && (q_cand - q_prev) * inv_norm + err_prev + err_cand <= LS_ACCEPT_RISE))
-        {
-            accepted = true;
-            taken = step;
-        }
+        ds_quadratic(A, R, X, a, mm, qc, ec, q_new, err_new);
+        if (tid == 0 && (!a.had_previous ||
+                         (a.norm_ok && (q_new - q_prev) * a.inv_norm + err_prev + err_new <= 1e-12)))
+            accepted = rung;
+        __syncthreads();
+        if (accepted >= 0)
+            break;
     }
-    g_ridge_tally[accepted ? taken : 3]++;
-    if (accepted)
+
+    if (accepted >= 0)
     {
-        for (int c = 0; c < nout; c++)
+        for (int e = tid; e < nout * mm; e += DS_THREADS)
+            out->x[e] = (float)X[e / mm][e % mm];
+        if (tid == 0)
+            out->rung = accepted;
+    }
+    else if (!a.had_previous)
+    {
+        // nothing usable and nothing to keep: the constant fit, each output's weighted mean target
+        const double count = A[nin][nin];
+        for (int e = tid; e < nout * mm; e += DS_THREADS)
         {
-            for (int i = 0; i < nin; i++)
-                m.dec_w[(size_t)c * nin + i] = (float)x_new[(size_t)c * mm + i];
-            m.dec_b[c] = (float)x_new[(size_t)c * mm + nin];
+            const int c = e / mm, i = e % mm;
+            out->x[e] = i < nin ? 0.0f : (count > 0.0 ? (float)(R[c][nin] / count) : 0.0f);
+        }
+        if (tid == 0)
+            out->rung = 3;
+    }
+    else if (tid == 0)
+        out->rung = 4;
+}
+
+static_assert(sizeof(DecoderSolveOut) <= 2048, "the arena's dec_solve slice holds one DecoderSolveOut");
+
+static long long g_rung_tally[4] = { 0, 0, 0, 0 };
+
+int solve_decoder_on_device(nntc_b200_device* d, nntc_b200_model& m, int k, const double* per_site)
+{
+    DecoderSolveArgs a{};
+    a.nin = m.nin;
+    a.nout = m.nout;
+    a.had_previous = m.has_decoder != 0;
+    double sum_cw = 0.0, sites = 0.0;
+    for (int c = 0; c < m.nout; c++)
+    {
+        a.cw[c] = m.cw[c];
+        sum_cw += (double)m.cw[c];
+        a.b[c] = m.dec_b[c];
+    }
+    for (int i = 0; i < m.nout * m.nin; i++)
+        a.w[i] = m.dec_w[i];
+    for (int i = 0; i < m.nplanes; i++)
+        sites += per_site[i] * (double)m.w0[i] * (double)m.h0[i] * (double)(1 + k);
+    a.norm_ok = sum_cw * sites > 0.0;
+    a.inv_norm = a.norm_ok ? 1.0 / (sum_cw * sites) : 0.0;
+    DecoderSolveOut* dev_out = reinterpret_cast<DecoderSolveOut*>(d->dec_solve);
+    k_decoder_solve<<<1, DS_THREADS, 0, d->stream>>>(d->reduction, a, dev_out);
+    NB_LAUNCHED();
+    DecoderSolveOut o;
+    NB_TRY(download(d, &o, dev_out, sizeof(o)));
+    const int mm = m.nin + 1;
+    g_rung_tally[o.rung < 3 ? o.rung : 3]++;
+    if (o.rung <= 3)
+    {
+        for (int c = 0; c < m.nout; c++)
+        {
+            for (int i = 0; i < m.nin; i++)
+                m.dec_w[c * m.nin + i] = o.x[c * mm + i];
+            m.dec_b[c] = o.x[c * mm + m.nin];
         }
         m.has_decoder = 1;
     }
-    else if (!had_previous)
-    {
-        for (int i = 0; i < nout * nin; i++)
-            m.dec_w[i] = 0.0f;
-        const double count = acc[(size_t)tri_index(nin, nin, mm)];
-        for (int c = 0; c < nout; c++)
-            m.dec_b[c] = count > 0.0 ? (float)(acc[(size_t)tri + (size_t)c * mm + nin] / count) : 0.0f;
-        m.has_decoder = 1;
-    }
-    return accepted ? taken : 3;
+    return NNTC_B200_OK;
 }
 
 }   // namespace nb
@@ -409,10 +536,7 @@ int nntc_b200_solve_decoder(nntc_b200_device* d, nntc_b200_model* m, int k, cons
 {
     double t = 0.0;
     NB_TRY(normal_equations(d, k, per_site, &t));
-    const int mm = d->nin + 1;
-    std::vector<double> acc((size_t)(mm * (mm + 1) / 2 + d->nout * mm));
-    NB_TRY(download(d, acc.data(), d->reduction, acc.size() * sizeof(double)));
-    decoder_from_normal_equations(*m, k, per_site, acc);
+    NB_TRY(solve_decoder_on_device(d, *m, k, per_site));
     NB_TRY(upload_decoder(d, m));
     if (ms)
         *ms = t;
@@ -422,7 +546,7 @@ int nntc_b200_solve_decoder(nntc_b200_device* d, nntc_b200_model* m, int k, cons
 void nntc_b200_decoder_ridge_tally(long long out[4])
 {
     for (int i = 0; i < 4; i++)
-        out[i] = g_ridge_tally[i];
+        out[i] = g_rung_tally[i];
 }
 
 }   // extern "C"

@@ -354,6 +354,7 @@ void layout(nntc_b200_device* d, const nntc_b200_model* m, Carver& take)
     const int mm = m->nin + 1;
     const size_t entries = (size_t)(mm * (mm + 1) / 2 + m->nout * mm);
     take(d->reduction, entries * sizeof(double));
+    take(d->dec_solve, 2048);
     // the normal equations' per-block partials of every plane, then one per-site weight per plane
     take(d->ls_partial, (d->planes.size() * entries * LS_GRID + MAX_PLANES) * sizeof(double));
     take(d->bc_stats, (size_t)MAX_PLANES * 2 * sizeof(double));

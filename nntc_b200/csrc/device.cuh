@@ -111,6 +111,7 @@ struct nntc_b200_device
     double* scalars = nullptr;           // MAX_PLANES * S_COUNT
     unsigned int* counters = nullptr;    // COUNTERS words
     double* reduction = nullptr;         // the normal equations of the last block (a)
+    void* dec_solve = nullptr;           // the device decoder solve's answer: the rung and the decoder (2 KB)
     double* ls_partial = nullptr;        // planes * entries * LS_GRID, then one weight per plane
     double* obj_partial = nullptr;       // 3 * MAX_PLANES * OBJ_GRID
     double* bc_stats = nullptr;          // MAX_PLANES * 2

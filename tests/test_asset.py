@@ -25,10 +25,11 @@ from PIL import Image
 
 from nntc_b200 import NntcError, abi, check, lib, materials
 from nntc_b200 import asset as A
+from conftest import reference_file
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "assets")
 CASES = json.load(open(os.path.join(GOLDEN, "cases.json")))
-REF_READER = "/root/reference/tools/dds_decode.py"
+REF_READER = reference_file("tools", "dds_decode.py")
 
 
 def indices_from_blocks(m, ep, sel):
@@ -174,7 +175,7 @@ def test_reference_reader_takes_the_rewritten_asset(tmp_path, case):
     assert len(quoted) == len(ours) and all(abs(a - b) <= 0.0051 for a, b in zip(ours, quoted)), (ours, quoted)
 
 
-REF_EXAMPLES = "/root/reference/examples"
+REF_EXAMPLES = reference_file("examples")
 SHIPPED = ["m1_m4_c0_3_c1_4", "pavingstones141_1k_c0_4"]
 
 

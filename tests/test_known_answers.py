@@ -10,8 +10,9 @@ import subprocess
 import pytest
 
 import oracle as O
+from conftest import reference_file
 
-TINY = "/root/reference/tests/tiny.png"
+TINY = reference_file("tests", "tiny.png")
 
 
 @pytest.mark.skipif(not (os.path.exists(O.REF_ENCODER) and os.path.exists(TINY)),
