@@ -299,7 +299,16 @@ enum nntc_b200_option
     /* 1: assemble the stencils with one thread per texel recomputing every site it touches, the reference's shape
      * (src/solve_level1.cu:259-581); 0 (default): one pass per site for the gradient terms, then one thread per
      * (texel, slot) for the monomial sums. */
-    NNTC_B200_OPT_REFERENCE_SHAPED_ASSEMBLY = 0
+    NNTC_B200_OPT_REFERENCE_SHAPED_ASSEMBLY = 0,
+    /* 1: block (a)'s normal equations on the tcgen05 tensor cores with the site rows split into BF16 hi + lo parts
+     * and FP32 accumulators, added in FP64 per 256 sites (the mixed-precision form; NOT the same bits: the sums hold
+     * to about 1e-6 relative); 0 (default): exact products summed in FP64 (src/solve_decoder.cu:87-161). */
+    NNTC_B200_OPT_MIXED_PRECISION_GRAM = 1,
+    /* 1: the conjugate gradients of blocks (b) and (c') apply (H + lambda I) matrix-free from the decode's forward pass
+     * and its adjoint in FP32, with FP64 inner products and recurrences, and stop at 1e-6 of the right-hand side; only
+     * the gradient and the diagonal blocks are assembled (the adjoint form; NOT the same bits). 0 (default): the
+     * assembled FP64 stencil (src/solve_level1.cu:781-828, 1222-1338). The quantised sweeps assemble in full either way. */
+    NNTC_B200_OPT_ADJOINT_CG = 2
 };
 int nntc_b200_set_option(nntc_b200_device* d, int option, int value);
 
@@ -313,9 +322,10 @@ enum nntc_b200_kernel
     NNTC_B200_K_NORMAL_EQ,       /* block (a)'s normal equations */
     NNTC_B200_K_ASSEMBLE1,       /* block (b)'s stencil and gradient gather */
     NNTC_B200_K_ASSEMBLE0,       /* block (c')'s stencil and gradient gather */
-    NNTC_B200_K_MATVEC,          /* one conjugate-gradient stencil mat-vec over every plane */
+    NNTC_B200_K_MATVEC,          /* one conjugate-gradient product over every plane, block (b) (level 1) */
     NNTC_B200_K_SWEEP,           /* one colour of the quantised sweeps */
     NNTC_B200_K_REFINE,          /* one colour of the BC refinement */
+    NNTC_B200_K_MATVEC0,         /* one conjugate-gradient product over every plane, block (c') (level 0) */
     NNTC_B200_K_COUNT
 };
 /* on != 0 brackets every launch of the kernels above with a pair of CUDA events; stats accumulate until reset. */

@@ -85,6 +85,12 @@ class EncodeResult(C.Structure):
                 ("ms_total", C.c_double), ("objective_passes", C.c_longlong)]
 
 
+# nntc_b200_set_option's options (include/nntc_b200.h, enum nntc_b200_option)
+OPT_REFERENCE_SHAPED_ASSEMBLY = 0
+OPT_MIXED_PRECISION_GRAM = 1
+OPT_ADJOINT_CG = 2
+
+
 def feature_count(c0: int, c1: int) -> int:
     return c1 + c0 + c0 * c1
 

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "device.cuh"
+#include "footprint.cuh"
 
 namespace nb
 {
@@ -214,61 +215,6 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
     A.y[A.site0[pl] + si] = make_float4(y[0], y[1], y[2], y[3]);
 }
 
-// The pixels whose bilinear footprint into an n1-wide plane can reach texel ti (src/solve_level1.cu:246-257).
-__host__ __device__ __forceinline__ void reach(int ti, int n0, int n1, int& lo, int& hi)
-{
-    const double r = (double)n0 / (double)n1;
-    lo = (int)ceil(((double)ti - 0.5) * r - 1.0);
-    hi = (int)ceil(((double)ti + 1.5) * r) - 1;
-    lo = lo < 0 ? 0 : lo;
-    hi = hi > n0 - 1 ? n0 - 1 : hi;
-}
-
-// Whether site (px, py, j) touches both texel (tx, ty) and texel (nbx, nby) of the unknown latent (w x h, its pixels
-// w0 x h0), and with which weights. A merged tap's weight is the sum, in corner order, of the corner weights that
-// landed on that texel (src/solve_level1.cu:287-316, 466-498): accumulating the corners of the self texel and of the
-// neighbour from zero gives the same two weights.
-template <bool LEVEL0>
-__host__ __device__ __forceinline__ bool site_touches(int px, int py, int j, int kc, int tx, int ty, int nbx, int nby,
-                                                      int w0, int h0, int w, int h, float& w_self, float& w_other)
-{
-    float dx, dy;
-    site_offset(kc, j, px, py, dx, dy);
-    w_self = 0.0f;
-    w_other = 0.0f;
-    bool has_self = false, has_other = false;
-    if (LEVEL0 && j == 0)
-    {
-        has_self = px == tx && py == ty;
-        has_other = px == nbx && py == nby;
-        w_self = has_self ? 1.0f : 0.0f;
-        w_other = has_other ? 1.0f : 0.0f;
-    }
-    else
-    {
-        const Tap tq = tap_at(px, py, dx, dy, w0, h0, w, h);
-        float cw4[4];
-        tap_weights(tq, cw4);
-        const int cx4[4] = { tq.x0, tq.x1, tq.x0, tq.x1 };
-        const int cy4[4] = { tq.y0, tq.y0, tq.y1, tq.y1 };
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-        {
-            if (cx4[q] == tx && cy4[q] == ty)
-            {
-                w_self += cw4[q];
-                has_self = true;
-            }
-            if (cx4[q] == nbx && cy4[q] == nby)
-            {
-                w_other += cw4[q];
-                has_other = true;
-            }
-        }
-    }
-    return has_self && has_other;
-}
-
 // ---- the gather's visit tables
 //
 // Away from the borders the sites that touch a texel and one of its neighbours, and their two weights, depend only on
@@ -351,6 +297,7 @@ struct GatherArgs
     unsigned tabled;      // bit i: plane i's interior texels may use the tables
     long long site0[MAX_PLANES + 1];
     long long bstart[MAX_PLANES + 1];   // each plane's first block
+    int slots;            // slots gathered: SLOTS, or 1 for the diagonal blocks and the gradient alone
 };
 
 // The texel at position `pos` of the stencil's colour-major order (the inverse of stencil_pos).
@@ -397,9 +344,9 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
     while (pl + 1 < P.n && A.bstart[pl + 1] <= (long long)blockIdx.x)
         pl++;
     const long long lb = (long long)blockIdx.x - A.bstart[pl];
-    const int slot = (int)(lb % SLOTS);
-    const int colour = (int)((lb / SLOTS) % 4);
-    const long long region = lb / SLOTS / 4;
+    const int slot = (int)(lb % A.slots);
+    const int colour = (int)((lb / A.slots) % 4);
+    const long long region = lb / A.slots / 4;
     const PlaneView& V = P.p[pl];
     const int tw_ = V.w, th_ = V.h;
     const long long w0c = (tw_ + 1) >> 1, w1c = tw_ >> 1, h0c = (th_ + 1) >> 1, h1c = th_ >> 1;
@@ -591,7 +538,8 @@ __global__ void __launch_bounds__(GATHER_THREADS, 7) k_gather_level1(Planes P, c
 }
 
 // Launch both passes for every plane: the per-site terms, then the per-(texel, slot) gather.
-int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono)
+int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono,
+                   int slots)
 {
     Planes S = planes_for(d, level0, [&](int i) {
         const DevPlane& p = d->planes[(size_t)i];
@@ -600,6 +548,7 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     S.kc = k;
     SiteArgs A{ d->site_terms, (float4*)d->site_y, {} };
     GatherArgs G{};
+    G.slots = slots;
     G.terms = d->site_terms;
     G.y = (const float4*)d->site_y;
     {
@@ -734,7 +683,7 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
         G.bstart[i] = blocks;
         const PlaneView& v = P_texels.p[i];
         const long long largest = (long long)((v.w + 1) / 2) * ((v.h + 1) / 2);   // colour 0
-        blocks += (largest + GATHER_THREADS - 1) / GATHER_THREADS * 4 * SLOTS;
+        blocks += (largest + GATHER_THREADS - 1) / GATHER_THREADS * 4 * slots;
     }
     G.bstart[P_texels.n] = blocks;
     const unsigned grid = (unsigned)blocks;

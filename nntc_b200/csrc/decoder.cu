@@ -22,11 +22,8 @@
 namespace nb
 {
 
-
-__host__ __device__ inline int tri_index(int i, int j, int mm)
-{
-    return i * mm - i * (i - 1) / 2 + (j - i);
-}
+size_t ls_tc_shared_bytes();
+int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries, cudaStream_t stream);
 
 struct LsArgs
 {
@@ -224,17 +221,38 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     P.kc = k;
     NB_TRY(block_begin(d));
     dim3 grid(LS_GRID, (unsigned)P.n);
-    const size_t shared = std::max((size_t)NE_THREADS * NE_STRIDE * sizeof(float),
-                                   (size_t)NE_WARPS * NE_TILES * 64 * sizeof(double));
-    NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
-    NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
-    k_ls_accumulate_mma<<<grid, NE_THREADS, shared, d->stream>>>(P, LsArgs{ d->ls_partial, entries });
-    NB_TRY(ktimer_end(d));
-    NB_LAUNCHED();
+    if (d->mixed_gram)
+    {
+        NB_CUDA(cudaMemsetAsync(d->counters + CNT_STATUS, 0, sizeof(unsigned int), d->stream));
+        NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
+        NB_TRY(launch_ls_accumulate_tc(d, P, d->ls_partial, entries, d->stream));
+        NB_TRY(ktimer_end(d));
+    }
+    else
+    {
+        const size_t shared = std::max((size_t)NE_THREADS * NE_STRIDE * sizeof(float),
+                                       (size_t)NE_WARPS * NE_TILES * 64 * sizeof(double));
+        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
+        NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
+        k_ls_accumulate_mma<<<grid, NE_THREADS, shared, d->stream>>>(P, LsArgs{ d->ls_partial, entries });
+        NB_TRY(ktimer_end(d));
+        NB_LAUNCHED();
+    }
     k_ls_reduce<<<grid_for((size_t)entries, 128), 128, 0, d->stream>>>(d->ls_partial, entries, P.n, omega,
                                                                       d->reduction);
     NB_LAUNCHED();
-    return block_end(d, ms);
+    NB_TRY(block_end(d, ms));
+    if (d->mixed_gram)
+    {
+        unsigned int status = 0;
+        NB_TRY(download(d, &status, d->counters + CNT_STATUS, sizeof(status)));
+        if (status)
+        {
+            set_error(NNTC_B200_ERR_TIMEOUT, "the tensor-core normal equations gave up waiting on their MMAs");
+            return NNTC_B200_ERR_TIMEOUT;
+        }
+    }
+    return NNTC_B200_OK;
 }
 
 // ---- the solve, on the device ---------------------------------------------------------------------------------------

@@ -375,10 +375,8 @@ void layout(nntc_b200_device* d, const nntc_b200_model* m, Carver& take)
     take(d->scratch, d->scratch_floats * sizeof(float));
     take(d->scratch8, d->scratch_bytes);
     take(d->rgb8, max0 * m->nout);
-    take(d->means, max1 * m->nout * sizeof(float));
-    if (m->init0_residual)
-        take(d->resid, max0 * m->nout * sizeof(float));
     take(d->cov, (size_t)(MAX_NOUT + MAX_NOUT * MAX_NOUT) * COV_GRID * sizeof(double));
+    take(d->basis, 1024);
     take(d->hist, (size_t)HIST_BINS * sizeof(unsigned long long));
     if (m->l0_bc8)
     {

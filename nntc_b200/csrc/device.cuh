@@ -56,7 +56,14 @@ constexpr int HIST_BINS = 4096;          // init0: the percentile histogram
 constexpr int CNT_SWEEP = 0;
 constexpr int CNT_SEARCH = 16;
 constexpr int CNT_ACTIVE = CNT_SEARCH + 4 * 16;
-constexpr int COUNTERS = CNT_ACTIVE + 16;
+constexpr int CNT_STATUS = CNT_ACTIVE + 16;   // the device status word: raised by a bounded wait that gave up
+constexpr int COUNTERS = CNT_STATUS + 1;
+
+// Entry (i, j), i <= j, of an m x m symmetric matrix's upper triangle stored row by row.
+__host__ __device__ inline int tri_index(int i, int j, int mm)
+{
+    return i * mm - i * (i - 1) / 2 + (j - i);
+}
 
 struct Work
 {
@@ -127,9 +134,10 @@ struct nntc_b200_device
     int gtab_kc[2] = { -1, -1 };         // the K each table was built for (-1: none yet)
     int gtab_off[2][4][6] = {};          // each table's entry ranges per parity class and slot
     int reference_shaped_assembly = 0;   // 1: the per-texel gather of the reference's shape (same bits, slower)
-    float* resid = nullptr;              // the widest plane's residual, nout per pixel (init0 residual only)
-    float* means = nullptr;              // the widest level-1 plane's block means, nout per texel
-    double* cov = nullptr;               // covariance partials (init)
+    int mixed_gram = 0;                  // 1: block (a)'s sums on the tensor cores, BF16 hi + lo (gram_tc.cu)
+    int adjoint_cg = 0;                  // 1: blocks (b) and (c')'s conjugate gradients matrix-free (adjoint_cg.cu)
+    double* cov = nullptr;               // the init's moment partials, [entry][COV_GRID]
+    void* basis = nullptr;               // the init's principal directions, peaks and divisor (1 KB)
     unsigned long long* hist = nullptr;  // the percentile histogram (init0, palette mode)
     float* scratch = nullptr;            // the largest plane's worth of floats (level 0 or level 1)
     uint8_t* scratch8 = nullptr;         // the largest plane's worth of bytes

@@ -1,17 +1,33 @@
-// init.cu: the initial state of both latents and their grids (src/init.cu:384-1400).
+// init.cu: the initial state of both latents and their grids (the method of src/init.cu:384-1400), on the device.
 //
-// - level 0: luma into channel 0 snapped to the palette, or continuous under --l0 bc8 (src/init.cu:389-482);
-// - level 1: the block mean of the source per level-1 texel, by source channel (box) or projected onto the base
-//   plane's principal directions (pca), fitted onto one min/max grid over the whole chain (src/init.cu:484-967);
-// - --init0 residual: one level-0 channel from the leading principal direction of the decode's residual, divided by
-//   its peak (bc8) or its 99th percentile (palette) over the chain (src/init.cu:969-1400);
-// - the grid fits: minmax or the 0.1 / 99.9 percentiles over every plane of the chain, then the snap onto the grid
-//   through the one definition of the grid value (src/init.cu:520-750).
+// - level 0: luma into channel 0 (2 luma - 1), the other channels zero; snapped to the nearest palette entry, or kept
+//   continuous under --l0 bc8;
+// - level 1, box: each texel the mean of its block of source pixels, channel c from source channel c (2 mean - 1);
+//   pca: the block means projected onto the leading principal directions of the base plane's block means, each
+//   component divided by its peak over the chain; then one min/max grid over the chain and the snap;
+// - --init0 residual: one level-0 channel from the leading principal direction of the decode's residual at the pixel
+//   centres (over the base plane, or the chain with each plane's site weight; by texture, the texture whose 3x3 block
+//   has the largest leading eigenvalue), divided by the projection's peak (bc8) or its 99th percentile (palette).
 //
-// The per-element kernels are the reference's arithmetic; the covariance sums are fixed-order two-stage reductions;
-// the eigenproblems, the sorts of the percentile fit and the histogram walk are small host work, as in the reference.
+// Shape on the B200. Nothing of the init leaves the device but the report's few numbers:
+// - moments (means and covariance sums) by k_moments: a block stages a tile of rows - block means or decode residuals,
+//   formed on the fly, never stored - in shared memory, and each thread owns one entry (a channel sum or one product
+//   of the upper triangle) over all of the block's tiles; one partial per block and entry, added in block order;
+// - the eigenproblem by k_basis, one block: a parallel (round-robin) Jacobi on the <= 18 x 18 covariance, every
+//   disjoint pair of a round rotated at once;
+// - projections, peaks (an integer max on the bits of non-negative doubles), the percentile histogram (integer
+//   counts) and the seeds by fused kernels that form each pixel's residual in registers; every plane of the chain in
+//   one launch where the work is per texel.
+//
+// What has to be alike, and why: the per-element arithmetic of the seeds (luma weights, block means in row order, the
+// decode at the pixel centre, the projection sum, the clamps and roundings) decides quantised values the reference's
+// check harness compares; the percentile rule (4096 bins of |p| / peak, the first bin whose running count reaches
+// 0.99 of all texels) and the sign rule of init0's direction (its largest entry positive) are the method's. A
+// principal direction's sign is not fixed by the method for level 1's pca components (the reference keeps whatever its
+// eigen solver returns); here each component gets the same rule as init0's direction.
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -22,54 +38,73 @@
 namespace nb
 {
 
+constexpr int MOM_TILE = 128;                                        // rows per staged tile
+constexpr int MOM_ENTRIES = MAX_NOUT + MAX_NOUT * (MAX_NOUT + 1) / 2;   // sums, then the upper triangle
+constexpr int JM = MAX_NOUT + 1;                                     // the eigen solver's padded order (even)
 
-struct ChannelBits
-{
-    int b[MAX_CH];
+// What k_basis hands to the projection kernels and back to the host.
+struct Basis
+{   // 808 bytes; the arena's slice is 1 KB
+    double mu[MAX_NOUT];
+    double dir[MAX_CH][MAX_NOUT];
+    double eig[MAX_CH];
+    double total_variance;
+    unsigned long long peak_bits[MAX_CH];   // max |projection| per component, as the bits of a non-negative double
+    double divisor;
+    int texture;
+    int bin;
 };
 
-__global__ void k_init_level0(const float* src, int w, int h, int nout, int c0, ChannelBits bits, const float* palette,
-                              float lr, float lg, float lb, int luma_channel0, float* v0, uint8_t* k0)
+static_assert(sizeof(Basis) <= 1024, "the arena's basis slice holds one Basis");
+
+// ---- level 0 -----------------------------------------------------------------------------------------------------
+
+struct SeedArgs
 {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)w * h)
+    float luma[3];
+    int luma_channel0;
+    int palette_mode;
+    int levels[MAX_CH];
+    const float* palette;
+};
+
+__global__ void k_seed_level0(Planes P, SeedArgs A)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pl = plane_of(P, i);
+    const PlaneView& V = P.p[pl];
+    const long long t = i - P.start[pl];
+    if (t >= (long long)V.w0 * V.h0)
         return;
-    const float* s = src + i * nout;
-    const float luma = lr * s[0] + lg * s[1] + lb * s[2];
-    for (int c = 0; c < c0; c++)
+    const float* s = V.src + t * P.nout;
+    const float luma = A.luma[0] * s[0] + A.luma[1] * s[1] + A.luma[2] * s[2];
+    for (int c = 0; c < P.c0; c++)
     {
-        const float value = (c == 0 && luma_channel0) ? 2.0f * luma - 1.0f : 0.0f;
-        const int levels = (1 << bits.b[c]) - 1;
+        const float want = (c == 0 && A.luma_channel0) ? 2.0f * luma - 1.0f : 0.0f;
         int k = 0;
-        float best = fabsf(palette[(size_t)c * 16] - value);
-        for (int j = 1; j <= levels; j++)
+        float v = want;
+        if (A.palette_mode)
         {
-            const float dist = fabsf(palette[(size_t)c * 16 + j] - value);
-            if (dist < best)
+            // the nearest entry of the channel's palette, the first of equals
+            const float* pal = A.palette + c * 16;
+            float gap = fabsf(pal[0] - want);
+            for (int j = 1; j <= A.levels[c]; j++)
             {
-                best = dist;
-                k = j;
+                const float g = fabsf(pal[j] - want);
+                k = g < gap ? j : k;
+                gap = g < gap ? g : gap;
             }
+            v = pal[k];
         }
-        v0[i * c0 + c] = palette[(size_t)c * 16 + k];
-        k0[i * c0 + c] = (uint8_t)k;
+        V.v0[t * P.c0 + c] = v;
+        V.k0[t * P.c0 + c] = (uint8_t)k;
     }
 }
 
-__global__ void k_init_level0_cont(const float* src, int w, int h, int nout, int c0, float lr, float lg, float lb,
-                                   int luma_channel0, float* v0)
-{
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)w * h)
-        return;
-    const float* s = src + i * nout;
-    const float luma = lr * s[0] + lg * s[1] + lb * s[2];
-    for (int c = 0; c < c0; c++)
-        v0[i * c0 + c] = (c == 0 && luma_channel0) ? 2.0f * luma - 1.0f : 0.0f;
-}
+// ---- level 1: block means ----------------------------------------------------------------------------------------
 
-// The footprint of level-1 texel (x, y): source pixels [x w0 / w1, (x + 1) w0 / w1) and the same in y.
-__device__ __forceinline__ void block_span(int x, int w0, int w1, int& a, int& b)
+// Source pixels [x w0 / w1, (x + 1) w0 / w1) of level-1 column x (at least one), and the same in y.
+__host__ __device__ __forceinline__ void block_span(int x, int w0, int w1, int& a, int& b)
 {
     a = (int)((long long)x * w0 / w1);
     b = (int)((long long)(x + 1) * w0 / w1);
@@ -78,374 +113,590 @@ __device__ __forceinline__ void block_span(int x, int w0, int w1, int& a, int& b
     b = b > w0 ? w0 : b;
 }
 
-__global__ void k_init_level1_box(const float* src, int w0, int h0, int nout, int w1, int h1, int c1, float* out)
+// The mean of the first n source channels over level-1 texel t's block, summed in row order.
+__device__ __forceinline__ void block_mean(const float* src, int w0, int h0, int nout, int w1, int h1, size_t t,
+                                           int n, float* out)
 {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)w1 * h1)
-        return;
-    const int x = (int)(i % (size_t)w1), y = (int)(i / (size_t)w1);
     int xa, xb, ya, yb;
-    block_span(x, w0, w1, xa, xb);
-    block_span(y, h0, h1, ya, yb);
-    float acc[MAX_CH];
-    for (int c = 0; c < c1; c++)
-        acc[c] = 0.0f;
-    int n = 0;
-    for (int sy = ya; sy < yb; sy++)
-        for (int sx = xa; sx < xb; sx++)
+    block_span((int)(t % (size_t)w1), w0, w1, xa, xb);
+    block_span((int)(t / (size_t)w1), h0, h1, ya, yb);
+    for (int c = 0; c < n; c++)
+        out[c] = 0.0f;
+    for (int y = ya; y < yb; y++)
+        for (int x = xa; x < xb; x++)
         {
-            const float* s = src + ((size_t)sy * w0 + sx) * nout;
-            for (int c = 0; c < c1; c++)
-                acc[c] += c < nout ? s[c] : 0.0f;
-            n++;
+            const float* s = src + ((size_t)y * w0 + x) * nout;
+            for (int c = 0; c < n; c++)
+                out[c] += s[c];
         }
-    const float inv = n > 0 ? 1.0f / (float)n : 0.0f;
-    for (int c = 0; c < c1; c++)
-        out[i * c1 + c] = c < nout ? 2.0f * acc[c] * inv - 1.0f : 0.0f;
+    const int count = (xb - xa) * (yb - ya);
+    const float inv = count > 0 ? 1.0f / (float)count : 0.0f;
+    for (int c = 0; c < n; c++)
+        out[c] *= inv;
 }
 
-__global__ void k_block_means(const float* src, int w0, int h0, int nout, int w1, int h1, float* means)
+__global__ void k_box_level1(Planes P)
 {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)w1 * h1)
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pl = plane_of(P, i);
+    const PlaneView& V = P.p[pl];
+    const long long t = i - P.start[pl];
+    if (t >= (long long)V.w1 * V.h1)
         return;
-    const int x = (int)(i % (size_t)w1), y = (int)(i / (size_t)w1);
-    int xa, xb, ya, yb;
-    block_span(x, w0, w1, xa, xb);
-    block_span(y, h0, h1, ya, yb);
-    float acc[MAX_NOUT];
-    for (int c = 0; c < nout; c++)
-        acc[c] = 0.0f;
-    int n = 0;
-    for (int sy = ya; sy < yb; sy++)
-        for (int sx = xa; sx < xb; sx++)
-        {
-            const float* s = src + ((size_t)sy * w0 + sx) * nout;
-            for (int c = 0; c < nout; c++)
-                acc[c] += s[c];
-            n++;
-        }
-    const float inv = n > 0 ? 1.0f / (float)n : 0.0f;
-    for (int c = 0; c < nout; c++)
-        means[i * (size_t)nout + c] = acc[c] * inv;
+    const int c1 = P.c1, n = c1 < P.nout ? c1 : P.nout;
+    float m[MAX_CH];
+    block_mean(V.src, V.w0, V.h0, P.nout, V.w1, V.h1, (size_t)t, n, m);
+    for (int c = 0; c < c1; c++)
+        V.v1[t * c1 + c] = c < n ? 2.0f * m[c] - 1.0f : 0.0f;
 }
 
-// Entry e < nout: the sum of channel e; entry nout + r nout + s: the sum of channel r times channel s. Block
-// (b, r) makes the partial b of the entries of channel r - its sum and its nout products - from ONE read of each row:
-// every entry's sum runs over the same texels in the same grid-stride order as one block per entry would, and is
-// folded by the same tree, so the partials do not depend on how entries share a block.
-__global__ void k_cov_partial(const float* v, size_t count, int nout, double* cov)
+// ---- rows for the moments -----------------------------------------------------------------------------------------
+
+struct MeanRows
 {
-    __shared__ double sh[256];
-    const int r = (int)blockIdx.y;
-    double acc[1 + MAX_NOUT];
-#pragma unroll
-    for (int q = 0; q <= MAX_NOUT; q++)
-        acc[q] = 0.0;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (size_t)gridDim.x * blockDim.x)
+    const float* src;
+    int w0, h0, w1, h1, nout;
+    __device__ void row(size_t t, float* out) const { block_mean(src, w0, h0, nout, w1, h1, t, nout, out); }
+};
+
+// The decode's residual at pixel t's centre: level 0 read nearest, level 1 bilinear at the centre, minus the source.
+struct ResidualRows
+{
+    float* v0;
+    uint8_t* k0;
+    const float *v1, *src, *weights, *bias;
+    int w0, h0, w1, h1, c0, c1, nin, nout;
+    __device__ void row(size_t t, float* out) const
     {
-        const float* row = v + t * (size_t)nout;
-        const double a = (double)row[r];
-        acc[0] += a;
-#pragma unroll
-        for (int q = 0; q < MAX_NOUT; q++)
-            if (q < nout)
-                acc[1 + q] += a * (double)row[q];
+        const int px = (int)(t % (size_t)w0), py = (int)(t / (size_t)w0);
+        float s[MAX_CH], c[MAX_CH], phi[MAX_NIN];
+        for (int i = 0; i < c0; i++)
+            s[i] = v0[t * c0 + i];
+        blend<MAX_CH>(v1, w1, c1, tap_at(px, py, 0.0f, 0.0f, w0, h0, w1, h1), c);
+        features(s, c0, c, c1, phi);
+        for (int r = 0; r < nout; r++)
+        {
+            const float* wr = weights + (size_t)r * nin;
+            float dec = bias[r];
+            for (int i = 0; i < nin; i++)
+                dec += wr[i] * phi[i];
+            out[r] = dec - src[t * nout + r];
+        }
     }
-#pragma unroll
-    for (int q = 0; q <= MAX_NOUT; q++)
+};
+
+// Entry e of the moments: e < nout the sum of channel e, then the products (a, b), a <= b, row by row.
+__host__ __device__ inline void moment_pair(int e, int nout, int& a, int& b)
+{
+    int k = e - nout;
+    a = 0;
+    while (k >= nout - a)
     {
-        if (q > nout)
-            break;
+        k -= nout - a;
+        a++;
+    }
+    b = a + k;
+}
+
+// partial[e][block] (COV_GRID blocks) = weight x the block's sum of entry e, added to what is there when `accumulate`.
+template <class Rows>
+__global__ void __launch_bounds__(256) k_moments(Rows R, size_t count, int nout, double weight, int accumulate,
+                                                 double* partial)
+{
+    __shared__ float rows[MOM_TILE][MAX_NOUT + 1];
+    const int entries = nout + nout * (nout + 1) / 2;
+    const int e = threadIdx.x;
+    int a = 0, b = 0;
+    if (e >= nout && e < entries)
+        moment_pair(e, nout, a, b);
+    double acc = 0.0;
+    for (size_t start = (size_t)blockIdx.x * MOM_TILE; start < count; start += (size_t)gridDim.x * MOM_TILE)
+    {
         __syncthreads();
-        sh[threadIdx.x] = acc[q];
-        __syncthreads();
-        for (int half = (int)blockDim.x / 2; half > 0; half >>= 1)
+        for (int r = threadIdx.x; r < MOM_TILE; r += blockDim.x)
         {
-            if ((int)threadIdx.x < half)
-                sh[threadIdx.x] += sh[threadIdx.x + half];
+            if (start + r < count)
+                R.row(start + r, rows[r]);
+            else
+                for (int c = 0; c < nout; c++)
+                    rows[r][c] = 0.0f;   // a padded row adds exact zeros
+        }
+        __syncthreads();
+        if (e < nout)
+            for (int r = 0; r < MOM_TILE; r++)
+                acc += (double)rows[r][e];
+        else if (e < entries)
+            for (int r = 0; r < MOM_TILE; r++)
+                acc += (double)rows[r][a] * (double)rows[r][b];
+    }
+    if (e < entries)
+    {
+        double* slot = partial + (size_t)e * COV_GRID + blockIdx.x;
+        *slot = accumulate ? *slot + weight * acc : weight * acc;
+    }
+}
+
+// ---- the basis: covariance, eigenproblem, choice of directions ---------------------------------------------------
+
+// Parallel Jacobi on the symmetric n x n matrix A (shared, padded to an even order m with zero rows): every round
+// rotates m / 2 disjoint pairs at once, the pairs of a round-robin tournament, m - 1 rounds a sweep. V accumulates the
+// rotations. Every thread of the block calls it.
+__device__ void jacobi_block(double (*A)[JM], double (*V)[JM], int n, double* cs, double* sn, double* red)
+{
+    const int m = n + (n & 1), half = m / 2, tid = threadIdx.x;
+    for (int e = tid; e < JM * JM; e += blockDim.x)
+    {
+        const int i = e / JM, j = e % JM;
+        V[i][j] = i == j ? 1.0 : 0.0;
+        if (i >= n || j >= n)
+            A[i][j] = 0.0;
+    }
+    __syncthreads();
+    for (int sweep = 0; sweep < 64; sweep++)
+    {
+        if (tid == 0)
+        {
+            double off = 0.0, diag = 0.0;
+            for (int p = 0; p < n; p++)
+            {
+                diag += A[p][p] * A[p][p];
+                for (int q = p + 1; q < n; q++)
+                    off += A[p][q] * A[p][q];
+            }
+            red[0] = off <= 1e-30 * diag || off == 0.0 ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        if (red[0] != 0.0)
+            break;
+        for (int round = 0; round < m - 1; round++)
+        {
+            // pair k of this round: the fixed player m - 1 meets player `round`; the others meet symmetrically
+            if (tid < half)
+            {
+                int p = tid == 0 ? m - 1 : (round + tid) % (m - 1);
+                int q = tid == 0 ? round : (round - tid + (m - 1)) % (m - 1);
+                if (p > q)
+                {
+                    const int x = p;
+                    p = q;
+                    q = x;
+                }
+                double c = 1.0, s = 0.0;
+                const double apq = A[p][q];
+                if (apq != 0.0)
+                {
+                    const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+                    const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                    c = 1.0 / sqrt(t * t + 1.0);
+                    s = t * c;
+                }
+                cs[tid] = c;
+                sn[tid] = s;
+                red[2 + 2 * tid] = p;
+                red[3 + 2 * tid] = q;
+            }
+            __syncthreads();
+            // columns: A <- A G, V <- V G
+            for (int w = tid; w < half * m; w += blockDim.x)
+            {
+                const int k = w / half, pr = w % half;
+                const int p = (int)red[2 + 2 * pr], q = (int)red[3 + 2 * pr];
+                const double c = cs[pr], s = sn[pr];
+                const double akp = A[k][p], akq = A[k][q];
+                A[k][p] = c * akp - s * akq;
+                A[k][q] = s * akp + c * akq;
+                const double vkp = V[k][p], vkq = V[k][q];
+                V[k][p] = c * vkp - s * vkq;
+                V[k][q] = s * vkp + c * vkq;
+            }
+            __syncthreads();
+            // rows: A <- G^T A
+            for (int w = tid; w < half * m; w += blockDim.x)
+            {
+                const int k = w / half, pr = w % half;
+                const int p = (int)red[2 + 2 * pr], q = (int)red[3 + 2 * pr];
+                const double c = cs[pr], s = sn[pr];
+                const double apk = A[p][k], aqk = A[q][k];
+                A[p][k] = c * apk - s * aqk;
+                A[q][k] = s * apk + c * aqk;
+            }
             __syncthreads();
         }
-        if (threadIdx.x == 0)
+    }
+}
+
+struct BasisArgs
+{
+    int nout;
+    int mode;         // 0: level 1's leading `components` directions; 1: init0's leading direction; 2: init0 by texture
+    int components;
+    int textures;
+    double count;     // the (weighted) number of rows the moments summed
+};
+
+// A direction with its largest entry (the first of equals in magnitude) made positive.
+__device__ void sign_rule(double* u, int n)
+{
+    int big = 0;
+    for (int r = 1; r < n; r++)
+        if (fabs(u[r]) > fabs(u[big]))
+            big = r;
+    if (u[big] < 0.0)
+        for (int r = 0; r < n; r++)
+            u[r] = -u[r];
+}
+
+__global__ void __launch_bounds__(256) k_basis(const double* partial, BasisArgs a, Basis* out)
+{
+    __shared__ double raw[MOM_ENTRIES];
+    __shared__ double C[JM][JM], A[JM][JM], V[JM][JM];
+    __shared__ double cs[JM / 2 + 1], sn[JM / 2 + 1], red[2 + JM + 2];
+    __shared__ double mu[MAX_NOUT];
+    const int nout = a.nout, tid = threadIdx.x;
+    const int entries = nout + nout * (nout + 1) / 2;
+    for (int e = tid; e < entries; e += blockDim.x)
+    {
+        double s = 0.0;
+        for (int b = 0; b < COV_GRID; b++)
+            s += partial[(size_t)e * COV_GRID + b];
+        raw[e] = s;
+    }
+    __syncthreads();
+    if (tid < nout)
+        mu[tid] = a.count > 0.0 ? raw[tid] / a.count : 0.0;
+    __syncthreads();
+    for (int e = nout + tid; e < entries; e += blockDim.x)
+    {
+        int p, q;
+        moment_pair(e, nout, p, q);
+        const double v = (a.count > 0.0 ? raw[e] / a.count : 0.0) - mu[p] * mu[q];
+        C[p][q] = v;
+        C[q][p] = v;
+    }
+    for (int e = tid; e < MAX_NOUT; e += blockDim.x)
+        out->mu[e] = e < nout ? mu[e] : 0.0;
+    __syncthreads();
+    if (tid == 0)
+    {
+        double tv = 0.0;
+        for (int r = 0; r < nout; r++)
+            tv += C[r][r];
+        out->total_variance = tv;
+        out->texture = -1;
+        for (int j = 0; j < MAX_CH; j++)
+            out->peak_bits[j] = 0ull;
+    }
+    if (a.mode < 2)
+    {
+        for (int e = tid; e < JM * JM; e += blockDim.x)
+            A[e / JM][e % JM] = C[e / JM][e % JM];
+        __syncthreads();
+        jacobi_block(A, V, nout, cs, sn, red);
+        if (tid == 0)
         {
-            const int e = q == 0 ? r : nout + r * nout + (q - 1);
-            cov[(size_t)e * COV_GRID + blockIdx.x] = sh[0];
+            // the leading directions by eigenvalue, largest first (the first index of equals)
+            bool used[JM] = {};
+            const int take = a.mode == 0 ? a.components : 1;
+            for (int j = 0; j < take; j++)
+            {
+                int top = -1;
+                for (int i = 0; i < nout; i++)
+                    if (!used[i] && (top < 0 || A[i][i] > A[top][top]))
+                        top = i;
+                used[top] = true;
+                double u[MAX_NOUT];
+                for (int r = 0; r < nout; r++)
+                    u[r] = V[r][top];
+                sign_rule(u, nout);
+                for (int r = 0; r < MAX_NOUT; r++)
+                    out->dir[j][r] = r < nout ? u[r] : 0.0;
+                out->eig[j] = A[top][top];
+            }
+        }
+    }
+    else
+    {
+        // by texture: the 3x3 block of each texture's own channels, the texture whose leading eigenvalue is largest
+        __shared__ double best_value, best_vec[3];
+        __shared__ int best_t;
+        if (tid == 0)
+        {
+            best_value = -1.0;
+            best_t = 0;
+        }
+        for (int t = 0; t < a.textures; t++)
+        {
+            __syncthreads();
+            for (int e = tid; e < JM * JM; e += blockDim.x)
+            {
+                const int i = e / JM, j = e % JM;
+                A[i][j] = i < 3 && j < 3 ? C[3 * t + i][3 * t + j] : 0.0;
+            }
+            __syncthreads();
+            jacobi_block(A, V, 3, cs, sn, red);
+            if (tid == 0)
+            {
+                int top = 0;
+                for (int i = 1; i < 3; i++)
+                    if (A[i][i] > A[top][top])
+                        top = i;
+                if (A[top][top] > best_value)
+                {
+                    best_value = A[top][top];
+                    best_t = t;
+                    for (int r = 0; r < 3; r++)
+                        best_vec[r] = V[r][top];
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            double u[MAX_NOUT];
+            for (int r = 0; r < nout; r++)
+                u[r] = 0.0;
+            for (int r = 0; r < 3; r++)
+                u[3 * best_t + r] = best_vec[r];
+            sign_rule(u, nout);
+            for (int r = 0; r < MAX_NOUT; r++)
+                out->dir[0][r] = r < nout ? u[r] : 0.0;
+            out->eig[0] = best_value > 0.0 ? best_value : 0.0;
+            out->texture = best_t;
         }
     }
 }
 
-__global__ void k_quantise(const float* in, size_t n, int c, int bits, const float* lo, const float* hi, float* v,
-                           uint8_t* k)
+__device__ __forceinline__ double project(const float* row, const Basis& B, int j, int nout)
+{
+    double acc = 0.0;
+    for (int r = 0; r < nout; r++)
+        acc += B.dir[j][r] * ((double)row[r] - B.mu[r]);
+    return acc;
+}
+
+__device__ __forceinline__ void peak_max(unsigned long long* bits, double v)
+{
+    atomicMax(bits, (unsigned long long)__double_as_longlong(v));   // v >= 0: the bits order as the values
+}
+
+// ---- level 1 pca: projections, peaks, normalisation ---------------------------------------------------------------
+
+__global__ void k_pca_project(Planes P, Basis* B, int components)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pl = plane_of(P, i);
+    const PlaneView& V = P.p[pl];
+    const long long t = i - P.start[pl];
+    if (t >= (long long)V.w1 * V.h1)
+        return;
+    float m[MAX_NOUT];
+    block_mean(V.src, V.w0, V.h0, P.nout, V.w1, V.h1, (size_t)t, P.nout, m);
+    for (int j = 0; j < P.c1; j++)
+    {
+        const double p = j < components ? project(m, *B, j, P.nout) : 0.0;
+        V.v1[t * P.c1 + j] = (float)p;
+        if (j < components)
+            peak_max(&B->peak_bits[j], fabs(p));
+    }
+}
+
+__global__ void k_pca_normalise(Planes P, const Basis* __restrict__ B)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pl = plane_of(P, i);
+    const PlaneView& V = P.p[pl];
+    const long long t = i - P.start[pl];
+    if (t >= (long long)V.w1 * V.h1)
+        return;
+    for (int j = 0; j < P.c1; j++)
+    {
+        const double peak = __longlong_as_double((long long)B->peak_bits[j]);
+        if (!(peak > 0.0))
+            continue;
+        const double v = (double)V.v1[t * P.c1 + j] * (1.0 / peak);
+        V.v1[t * P.c1 + j] = (float)(v < -1.0 ? -1.0 : (v > 1.0 ? 1.0 : v));
+    }
+}
+
+// ---- init0: peak, percentile histogram, divisor, seed -------------------------------------------------------------
+
+enum ResidualPass
+{
+    RP_PEAK = 0,
+    RP_HIST,
+    RP_SEED
+};
+
+struct ResidualPassArgs
+{
+    int channel, levels, palette_mode;
+    const float* palette;
+    unsigned long long* hist;
+};
+
+template <int PASS>
+__global__ void k_residual_pass(ResidualRows R, size_t texels, Basis* B, ResidualPassArgs a)
+{
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= texels)
+        return;
+    float row[MAX_NOUT];
+    R.row(t, row);
+    const double p = project(row, *B, 0, R.nout);
+    if (PASS == RP_PEAK)
+        peak_max(&B->peak_bits[0], fabs(p));
+    else if (PASS == RP_HIST)
+    {
+        const double peak = __longlong_as_double((long long)B->peak_bits[0]);
+        if (!(peak > 0.0))
+            return;
+        int b = (int)(fabs(p) * (1.0 / peak) * (double)HIST_BINS);
+        b = b < 0 ? 0 : (b >= HIST_BINS ? HIST_BINS - 1 : b);
+        atomicAdd(a.hist + b, 1ull);
+    }
+    else
+    {
+        const double inv = B->divisor > 0.0 ? 1.0 / B->divisor : 0.0;
+        const double q = p * inv;
+        const float value = (float)(q < -1.0 ? -1.0 : (q > 1.0 ? 1.0 : q));
+        float* v0 = R.v0;
+        if (a.palette_mode)
+        {
+            int k = (int)lroundf((value + 1.0f) * 0.5f * (float)a.levels);
+            k = k < 0 ? 0 : (k > a.levels ? a.levels : k);
+            v0[t * R.c0 + a.channel] = a.palette[a.channel * 16 + k];
+            R.k0[t * R.c0 + a.channel] = (uint8_t)k;
+        }
+        else
+            v0[t * R.c0 + a.channel] = value;
+    }
+}
+
+// The divisor: the peak under bc8; under palette the peak scaled to the first histogram bin whose running count
+// reaches 0.99 of every texel of the chain (the peak again if that is not positive).
+__global__ void __launch_bounds__(256) k_divisor(Basis* B, const unsigned long long* hist, unsigned long long total,
+                                                 int use_hist)
+{
+    __shared__ unsigned long long part[256];
+    __shared__ int first;
+    const int tid = threadIdx.x, per = HIST_BINS / 256;
+    const double peak = __longlong_as_double((long long)B->peak_bits[0]);
+    if (!use_hist || !(peak > 0.0))
+    {
+        if (tid == 0)
+        {
+            B->divisor = peak;
+            B->bin = HIST_BINS - 1;
+        }
+        return;
+    }
+    unsigned long long s = 0ull;
+    for (int b = 0; b < per; b++)
+        s += hist[tid * per + b];
+    part[tid] = s;
+    if (tid == 0)
+        first = HIST_BINS - 1;
+    __syncthreads();
+    if (tid == 0)
+    {
+        unsigned long long run = 0ull;
+        for (int i = 0; i < 256; i++)
+        {
+            const unsigned long long x = part[i];
+            part[i] = run;   // exclusive prefix
+            run += x;
+        }
+    }
+    __syncthreads();
+    const unsigned long long want = (unsigned long long)(0.99 * (double)total);
+    unsigned long long run = part[tid];
+    for (int b = 0; b < per; b++)
+    {
+        run += hist[tid * per + b];
+        if (run >= want)
+        {
+            atomicMin(&first, tid * per + b);
+            break;
+        }
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        double d = peak * (double)(first + 1) / (double)HIST_BINS;
+        B->divisor = d > 0.0 ? d : peak;
+        B->bin = first;
+    }
+}
+
+// ---- grids --------------------------------------------------------------------------------------------------------
+
+__global__ void k_snap(float* v, uint8_t* k, size_t n, int c, int bits, const float* lo, const float* hi)
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const int ch = (int)(i % (size_t)c);
-    const int kk = grid_index(lo[ch], hi[ch], bits, in[i]);
-    v[i] = grid_value(lo[ch], hi[ch], bits, kk);
-    k[i] = (uint8_t)kk;
-}
-
-__global__ void k_residual(const float* v0, const float* v1, const float* src, int w0, int h0, int w1, int h1, int c0,
-                           int c1, int nin, int nout, const float* weights, const float* bias, float* resid)
-{
-    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (size_t)w0 * h0)
-        return;
-    const int px = (int)(idx % (size_t)w0), py = (int)(idx / (size_t)w0);
-    float s[MAX_CH], c[MAX_CH], phi[MAX_NIN];
-    for (int i = 0; i < c0; i++)
-        s[i] = v0[idx * c0 + i];
-    const Tap t = tap_at(px, py, 0.0f, 0.0f, w0, h0, w1, h1);
-    blend<MAX_CH>(v1, w1, c1, t, c);
-    features(s, c0, c, c1, phi);
-    for (int r = 0; r < nout; r++)
-    {
-        float acc = bias[r];
-        const float* row = weights + (size_t)r * nin;
-        for (int i = 0; i < nin; i++)
-            acc += row[i] * phi[i];
-        resid[idx * (size_t)nout + r] = acc - src[idx * (size_t)nout + r];
-    }
-}
-
-struct ProjDir
-{
-    double e[MAX_NOUT];
-    double mu[MAX_NOUT];
-};
-
-__device__ __forceinline__ double proj_value(const float* resid, size_t t, int nout, const ProjDir& dir)
-{
-    double acc = 0.0;
-    for (int r = 0; r < nout; r++)
-        acc += dir.e[r] * ((double)resid[t * (size_t)nout + r] - dir.mu[r]);
-    return acc;
-}
-
-__global__ void k_proj_peak(const float* resid, size_t texels, int nout, ProjDir dir, double* partial)
-{
-    __shared__ double sh[256];
-    double acc = 0.0;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < texels; t += (size_t)gridDim.x * blockDim.x)
-    {
-        const double v = fabs(proj_value(resid, t, nout, dir));
-        acc = v > acc ? v : acc;
-    }
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int half = (int)blockDim.x / 2; half > 0; half >>= 1)
-    {
-        if ((int)threadIdx.x < half)
-            sh[threadIdx.x] = sh[threadIdx.x] > sh[threadIdx.x + half] ? sh[threadIdx.x] : sh[threadIdx.x + half];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        partial[blockIdx.x] = sh[0];
-}
-
-__global__ void k_proj_hist(const float* resid, size_t texels, int nout, ProjDir dir, double inv_peak, int bins,
-                            unsigned long long* hist)
-{
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < texels; t += (size_t)gridDim.x * blockDim.x)
-    {
-        const double v = fabs(proj_value(resid, t, nout, dir)) * inv_peak;
-        int b = (int)(v * (double)bins);
-        b = b < 0 ? 0 : (b >= bins ? bins - 1 : b);
-        atomicAdd(hist + b, 1ull);
-    }
-}
-
-__global__ void k_seed_channel(const float* resid, size_t texels, int nout, ProjDir dir, double inv, int c0,
-                               int channel, int levels, const float* palette, int palette_mode, float* v0, uint8_t* k0)
-{
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= texels)
-        return;
-    const double p = proj_value(resid, t, nout, dir) * inv;
-    const float value = (float)(p < -1.0 ? -1.0 : (p > 1.0 ? 1.0 : p));
-    if (palette_mode)
-    {
-        int k = (int)lroundf((value + 1.0f) * 0.5f * (float)levels);
-        k = k < 0 ? 0 : (k > levels ? levels : k);
-        v0[t * (size_t)c0 + channel] = palette[(size_t)channel * 16 + k];
-        k0[t * (size_t)c0 + channel] = (uint8_t)k;
-    }
-    else
-        v0[t * (size_t)c0 + channel] = value;
-}
-
-// ---- host helpers -------------------------------------------------------------------------------------------------
-
-static void fit_range(const std::vector<std::vector<float>>& cont, int nc, bool pct, std::vector<float>& lo,
-                      std::vector<float>& hi)
-{
-    lo.assign((size_t)nc, 1e30f);
-    hi.assign((size_t)nc, -1e30f);
-    if (!pct)
-    {
-        for (size_t i = 0; i < cont.size(); i++)
-            for (size_t t = 0; t < cont[i].size(); t++)
-            {
-                const int c = (int)(t % (size_t)nc);
-                lo[(size_t)c] = std::min(lo[(size_t)c], cont[i][t]);
-                hi[(size_t)c] = std::max(hi[(size_t)c], cont[i][t]);
-            }
-        return;
-    }
-    std::vector<float> v;
-    for (int c = 0; c < nc; c++)
-    {
-        v.clear();
-        for (size_t i = 0; i < cont.size(); i++)
-            for (size_t t = (size_t)c; t < cont[i].size(); t += (size_t)nc)
-                v.push_back(cont[i][t]);
-        if (v.empty())
-            continue;
-        const size_t last = v.size() - 1;
-        const size_t a = (size_t)(0.001 * (double)last + 0.5);
-        const size_t b = (size_t)(0.999 * (double)last + 0.5);
-        // the two order statistics of the sorted values, by selection
-        std::nth_element(v.begin(), v.begin() + (long)a, v.end());
-        lo[(size_t)c] = v[a];
-        std::nth_element(v.begin(), v.begin() + (long)b, v.end());
-        hi[(size_t)c] = v[b];
-    }
-}
-
-static void jacobi_eigen(std::vector<double>& a, int n, std::vector<double>& vec, std::vector<double>& val)
-{
-    vec.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; i++)
-        vec[(size_t)i * n + i] = 1.0;
-    for (int sweep = 0; sweep < 100; sweep++)
-    {
-        double off = 0.0;
-        for (int p = 0; p < n; p++)
-            for (int q = p + 1; q < n; q++)
-                off += a[(size_t)p * n + q] * a[(size_t)p * n + q];
-        if (off <= 1e-30)
-            break;
-        for (int p = 0; p < n; p++)
-            for (int q = p + 1; q < n; q++)
-            {
-                const double apq = a[(size_t)p * n + q];
-                if (std::fabs(apq) <= 1e-300)
-                    continue;
-                const double theta = (a[(size_t)q * n + q] - a[(size_t)p * n + p]) / (2.0 * apq);
-                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-                for (int k = 0; k < n; k++)
-                {
-                    const double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
-                    a[(size_t)k * n + p] = c * akp - s * akq;
-                    a[(size_t)k * n + q] = s * akp + c * akq;
-                }
-                for (int k = 0; k < n; k++)
-                {
-                    const double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
-                    a[(size_t)p * n + k] = c * apk - s * aqk;
-                    a[(size_t)q * n + k] = s * apk + c * aqk;
-                }
-                for (int k = 0; k < n; k++)
-                {
-                    const double vkp = vec[(size_t)k * n + p], vkq = vec[(size_t)k * n + q];
-                    vec[(size_t)k * n + p] = c * vkp - s * vkq;
-                    vec[(size_t)k * n + q] = s * vkp + c * vkq;
-                }
-            }
-    }
-    val.assign((size_t)n, 0.0);
-    for (int i = 0; i < n; i++)
-        val[(size_t)i] = a[(size_t)i * n + i];
-}
-
-// The covariance sums of `count` rows of nout floats on the device, added on the host in block order.
-static int cov_sums(nntc_b200_device* d, const float* rows, size_t count, int nout, std::vector<double>& raw)
-{
-    const int entries = nout + nout * nout;
-    dim3 grid((unsigned)COV_GRID, (unsigned)nout);
-    k_cov_partial<<<grid, 256, 0, d->stream>>>(rows, count, nout, d->cov);
-    NB_LAUNCHED();
-    std::vector<double> partial((size_t)entries * COV_GRID);
-    NB_TRY(download(d, partial.data(), d->cov, partial.size() * sizeof(double)));
-    raw.assign((size_t)entries, 0.0);
-    for (int e = 0; e < entries; e++)
-        for (int b = 0; b < COV_GRID; b++)
-            raw[(size_t)e] += partial[(size_t)e * COV_GRID + b];
-    return NNTC_B200_OK;
+    const int q = grid_index(lo[ch], hi[ch], bits, v[i]);
+    v[i] = grid_value(lo[ch], hi[ch], bits, q);
+    k[i] = (uint8_t)q;
 }
 
 int fit_grid_device(nntc_b200_device* d, int level0, bool pct, float* lo, float* hi);
 
-// Fit the grid (when `fit`) and snap every plane onto it. With `cont` empty both read the planes where the device holds
-// them; with a host copy (the pca init's projections) the fit is the host's and the snap reads the copy.
-static int fit_and_snap(nntc_b200_device* d, nntc_b200_model* m, int level0,
-                        const std::vector<std::vector<float>>& cont, bool pct, uint8_t* const* k_out, bool fit)
+// Fit the latent's grid over the chain where the device holds it (when `fit`), then snap every plane onto it.
+static int fit_and_snap(nntc_b200_device* d, nntc_b200_model* m, int level0, bool pct, uint8_t* const* k_out, bool fit)
 {
     const int nc = level0 ? d->c0 : d->c1;
     if (fit)
     {
-        std::vector<float> lo(MAX_CH), hi(MAX_CH);
-        if (cont.empty())
-            NB_TRY(fit_grid_device(d, level0, pct, lo.data(), hi.data()));   // the planes as the device holds them
-        else
-            fit_range(cont, nc, pct, lo, hi);
-        for (int c = 0; c < nc; c++)
-            if (!(hi[(size_t)c] > lo[(size_t)c]))
-            {
-                lo[(size_t)c] = -1.0f;
-                hi[(size_t)c] = 1.0f;
-            }
+        float lo[MAX_CH], hi[MAX_CH];
+        NB_TRY(fit_grid_device(d, level0, pct, lo, hi));
         for (int c = 0; c < nc; c++)
         {
-            if (level0)
+            if (!(hi[c] > lo[c]))
             {
-                m->lo0[c] = lo[(size_t)c];
-                m->hi0[c] = hi[(size_t)c];
+                lo[c] = -1.0f;
+                hi[c] = 1.0f;
             }
-            else
-            {
-                m->lo1[c] = lo[(size_t)c];
-                m->hi1[c] = hi[(size_t)c];
-            }
+            (level0 ? m->lo0 : m->lo1)[c] = lo[c];
+            (level0 ? m->hi0 : m->hi1)[c] = hi[c];
         }
-        if (level0)
-            m->has_lo0 = 1;
-        else
-            m->has_lo1 = 1;
+        (level0 ? m->has_lo0 : m->has_lo1) = 1;
         NB_TRY(upload_grids(d, m));
     }
     for (size_t i = 0; i < d->planes.size(); i++)
     {
         const DevPlane& p = d->planes[i];
         const size_t n = level0 ? (size_t)p.w0 * p.h0 * d->c0 : (size_t)p.w1 * p.h1 * d->c1;
-        float* v = level0 ? p.v0 : p.v1;
         uint8_t* k = level0 ? p.k0 : p.k1;
-        const float* in = v;   // snap in place (each thread reads and writes one value)
-        if (!cont.empty())
-        {
-            NB_TRY(upload(d, d->scratch, cont[i].data(), n * sizeof(float)));
-            in = d->scratch;
-        }
-        k_quantise<<<grid_for(n, 256), 256, 0, d->stream>>>(in, n, nc, level0 ? 8 : m->bits1, level0 ? d->lo0 : d->lo1,
-                                                           level0 ? d->hi0 : d->hi1, v, k);
+        k_snap<<<grid_for(n, 256), 256, 0, d->stream>>>(level0 ? p.v0 : p.v1, k, n, nc, level0 ? 8 : m->bits1,
+                                                        level0 ? d->lo0 : d->lo1, level0 ? d->hi0 : d->hi1);
         NB_LAUNCHED();
         if (k_out && k_out[i])
-            NB_TRY(download(d, k_out[i], k, n));
+            NB_CUDA(cudaMemcpyAsync(k_out[i], k, n, cudaMemcpyDeviceToHost, d->stream));
     }
     NB_CUDA(cudaStreamSynchronize(d->stream));
     return NNTC_B200_OK;
 }
 
-static int residual_pass(nntc_b200_device* d, size_t plane)
+static ResidualRows residual_rows(const nntc_b200_device* d, const DevPlane& p)
 {
-    const DevPlane& p = d->planes[plane];
-    const size_t n = (size_t)p.w0 * p.h0;
-    k_residual<<<grid_for(n, 256), 256, 0, d->stream>>>(p.v0, p.v1, p.src, p.w0, p.h0, p.w1, p.h1, d->c0, d->c1,
-                                                       d->nin, d->nout, d->weights, d->bias, d->resid);
-    NB_LAUNCHED();
-    return NNTC_B200_OK;
+    ResidualRows R{};
+    R.v0 = p.v0;
+    R.k0 = p.k0;
+    R.v1 = p.v1;
+    R.src = p.src;
+    R.weights = d->weights;
+    R.bias = d->bias;
+    R.w0 = p.w0;
+    R.h0 = p.h0;
+    R.w1 = p.w1;
+    R.h1 = p.h1;
+    R.c0 = d->c0;
+    R.c1 = d->c1;
+    R.nin = d->nin;
+    R.nout = d->nout;
+    return R;
 }
 
 }   // namespace nb
@@ -459,33 +710,21 @@ int nntc_b200_init_level0(nntc_b200_device* d, const nntc_b200_model* m, const f
                           uint8_t* const* k0_out)
 {
     NB_TRY(upload_grids(d, m));
-    ChannelBits bits{};
+    SeedArgs A{};
+    for (int i = 0; i < 3; i++)
+        A.luma[i] = luma[i];
+    A.luma_channel0 = luma_channel0 ? 1 : 0;
+    A.palette_mode = m->l0_bc8 ? 0 : 1;
     for (int c = 0; c < d->c0; c++)
-        bits.b[c] = m->bits0[c];
+        A.levels[c] = (1 << m->bits0[c]) - 1;
+    A.palette = d->palette;
+    Planes P = planes_for(d, 1, [&](int i) { return (size_t)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0; });
+    k_seed_level0<<<(unsigned)(P.start[P.n] / THREADS), THREADS, 0, d->stream>>>(P, A);
+    NB_LAUNCHED();
     for (size_t i = 0; i < d->planes.size(); i++)
-    {
-        const DevPlane& p = d->planes[i];
-        const size_t n = (size_t)p.w0 * p.h0;
-        if (m->l0_bc8)
-        {
-            k_init_level0_cont<<<grid_for(n, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, d->nout, d->c0, luma[0],
-                                                                        luma[1], luma[2], luma_channel0 ? 1 : 0,
-                                                                        p.v0);
-            NB_LAUNCHED();
-            NB_CUDA(cudaMemsetAsync(p.k0, 0, n * d->c0, d->stream));
-            if (k0_out && k0_out[i])
-                std::memset(k0_out[i], 0, n * d->c0);
-        }
-        else
-        {
-            k_init_level0<<<grid_for(n, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, d->nout, d->c0, bits,
-                                                                   d->palette, luma[0], luma[1], luma[2],
-                                                                   luma_channel0 ? 1 : 0, p.v0, p.k0);
-            NB_LAUNCHED();
-            if (k0_out && k0_out[i])
-                NB_TRY(download(d, k0_out[i], p.k0, n * d->c0));
-        }
-    }
+        if (k0_out && k0_out[i])
+            NB_CUDA(cudaMemcpyAsync(k0_out[i], d->planes[i].k0, (size_t)d->planes[i].w0 * d->planes[i].h0 * d->c0,
+                                    cudaMemcpyDeviceToHost, d->stream));
     NB_CUDA(cudaStreamSynchronize(d->stream));
     return NNTC_B200_OK;
 }
@@ -495,298 +734,172 @@ int nntc_b200_init_level1(nntc_b200_device* d, nntc_b200_model* m, int pca, nntc
 {
     *rep = nntc_b200_init1_report{};
     rep->pca = pca;
-    std::vector<std::vector<float>> cont(d->planes.size());
-    const int c1 = d->c1, nout = d->nout;
+    const int nout = d->nout;
+    Planes P = planes_for(d, 0, [&](int i) { return (size_t)d->planes[(size_t)i].w1 * d->planes[(size_t)i].h1; });
+    const unsigned blocks = (unsigned)(P.start[P.n] / THREADS);
     if (!pca)
     {
-        for (size_t i = 0; i < d->planes.size(); i++)
-        {
-            const DevPlane& p = d->planes[i];
-            const size_t n = (size_t)p.w1 * p.h1;
-            k_init_level1_box<<<grid_for(n, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, nout, p.w1, p.h1, c1, p.v1);
-            NB_LAUNCHED();
-        }
-        const std::vector<std::vector<float>> on_device;
-        return fit_and_snap(d, m, 0, on_device, false, k1_out, true);
-    }
-    // The basis: the base plane's block means, their covariance, the host eigenproblem.
-    std::vector<double> raw;
-    {
-        const DevPlane& p = d->planes[0];
-        const size_t texels = (size_t)p.w1 * p.h1;
-        k_block_means<<<grid_for(texels, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, nout, p.w1, p.h1, d->means);
+        k_box_level1<<<blocks, THREADS, 0, d->stream>>>(P);
         NB_LAUNCHED();
-        NB_TRY(cov_sums(d, d->means, texels, nout, raw));
+        return fit_and_snap(d, m, 0, false, k1_out, true);
     }
+    // the basis from the base plane's block means, then every plane projected onto it, on the device
     const DevPlane& base = d->planes[0];
-    const double count = (double)((size_t)base.w1 * base.h1);
-    std::vector<double> mu((size_t)nout, 0.0), cov((size_t)nout * nout, 0.0);
-    for (int r = 0; r < nout; r++)
-        mu[(size_t)r] = count > 0.0 ? raw[(size_t)r] / count : 0.0;
-    for (int r = 0; r < nout; r++)
-        for (int s = 0; s < nout; s++)
-            cov[(size_t)r * nout + s] =
-                (count > 0.0 ? raw[(size_t)(nout + r * nout + s)] / count : 0.0) - mu[(size_t)r] * mu[(size_t)s];
-    for (int r = 0; r < nout; r++)
-        rep->total_variance += cov[(size_t)r * nout + r];
-    std::vector<double> work = cov, vec, val;
-    jacobi_eigen(work, nout, vec, val);
-    std::vector<int> order((size_t)nout);
-    for (int i = 0; i < nout; i++)
-        order[(size_t)i] = i;
-    std::sort(order.begin(), order.end(), [&](int a, int b) { return val[(size_t)a] > val[(size_t)b]; });
-    rep->components = c1 < nout ? c1 : nout;
-    for (int j = 0; j < rep->components && j < MAX_CH; j++)
-        rep->eigenvalue[j] = val[(size_t)order[(size_t)j]];
-    std::vector<float> means;
-    std::vector<double> peak((size_t)c1, 0.0);
-    for (size_t i = 0; i < d->planes.size(); i++)
+    const size_t count = (size_t)base.w1 * base.h1;
+    MeanRows R{ base.src, base.w0, base.h0, base.w1, base.h1, nout };
+    k_moments<MeanRows><<<COV_GRID, 256, 0, d->stream>>>(R, count, nout, 1.0, 0, d->cov);
+    NB_LAUNCHED();
+    BasisArgs a{};
+    a.nout = nout;
+    a.mode = 0;
+    a.components = d->c1 < nout ? d->c1 : nout;
+    a.textures = m->textures;
+    a.count = (double)count;
+    Basis* B = reinterpret_cast<Basis*>(d->basis);
+    k_basis<<<1, 256, 0, d->stream>>>(d->cov, a, B);
+    NB_LAUNCHED();
+    k_pca_project<<<blocks, THREADS, 0, d->stream>>>(P, B, a.components);
+    NB_LAUNCHED();
+    k_pca_normalise<<<blocks, THREADS, 0, d->stream>>>(P, B);
+    NB_LAUNCHED();
+    Basis h;
+    NB_TRY(download(d, &h, B, sizeof(h)));
+    rep->components = a.components;
+    rep->total_variance = h.total_variance;
+    for (int j = 0; j < a.components && j < MAX_CH; j++)
     {
-        const DevPlane& p = d->planes[i];
-        const size_t texels = (size_t)p.w1 * p.h1;
-        k_block_means<<<grid_for(texels, 256), 256, 0, d->stream>>>(p.src, p.w0, p.h0, nout, p.w1, p.h1, d->means);
-        NB_LAUNCHED();
-        means.resize(texels * (size_t)nout);
-        NB_TRY(download(d, means.data(), d->means, means.size() * sizeof(float)));
-        cont[i].assign(texels * (size_t)c1, 0.0f);
-        for (size_t t = 0; t < texels; t++)
-            for (int j = 0; j < rep->components; j++)
-            {
-                const int col = order[(size_t)j];
-                double acc = 0.0;
-                for (int r = 0; r < nout; r++)
-                    acc += vec[(size_t)r * nout + col] * ((double)means[t * (size_t)nout + r] - mu[(size_t)r]);
-                cont[i][t * (size_t)c1 + j] = (float)acc;
-                peak[(size_t)j] = std::max(peak[(size_t)j], std::fabs(acc));
-            }
+        rep->eigenvalue[j] = h.eig[j];
+        double peak;
+        std::memcpy(&peak, &h.peak_bits[j], sizeof(peak));
+        rep->peak[j] = peak;
     }
-    for (int j = 0; j < c1; j++)
-    {
-        rep->peak[j] = peak[(size_t)j];
-        if (!(peak[(size_t)j] > 0.0))
-            continue;
-        const double inv = 1.0 / peak[(size_t)j];
-        for (size_t i = 0; i < cont.size(); i++)
-            for (size_t t = (size_t)j; t < cont[i].size(); t += (size_t)c1)
-            {
-                const double v = (double)cont[i][t] * inv;
-                cont[i][t] = (float)(v < -1.0 ? -1.0 : (v > 1.0 ? 1.0 : v));
-            }
-    }
-    return fit_and_snap(d, m, 0, cont, false, k1_out, true);
+    return fit_and_snap(d, m, 0, false, k1_out, true);
 }
 
 int nntc_b200_init0_residual_channel(nntc_b200_device* d, const nntc_b200_model* m, int channel,
                                      const double* plane_weight, nntc_b200_init0_report* rep, uint8_t* const* k0_io)
 {
-    if (!d->resid)
+    if (channel < 0 || channel >= d->c0)
     {
-        set_error(NNTC_B200_ERR_STATE, "the residual seed needs a model created with init0_residual");
-        return NNTC_B200_ERR_STATE;
+        set_error(NNTC_B200_ERR_ARG, "init0 channel out of range");
+        return NNTC_B200_ERR_ARG;
     }
     const int nout = d->nout;
     *rep = nntc_b200_init0_report{};
     rep->nout = nout;
     rep->texture = -1;
-    const int entries = nout + nout * nout;
-    std::vector<double> raw((size_t)entries, 0.0);
+    // the residual's moments: the base plane, or every plane of the chain with its site weight
     double count = 0.0;
-    {
-        const size_t nplanes = m->init0_chain ? d->planes.size() : 1;
-        for (size_t i = 0; i < nplanes; i++)
-        {
-            const DevPlane& p = d->planes[i];
-            const size_t texels = (size_t)p.w0 * p.h0;
-            const double w = m->init0_chain ? plane_weight[i] : 1.0;
-            if (!(w > 0.0))
-                continue;
-            NB_TRY(residual_pass(d, i));
-            std::vector<double> part;
-            NB_TRY(cov_sums(d, d->resid, texels, nout, part));
-            for (int e = 0; e < entries; e++)
-                raw[(size_t)e] += w * part[(size_t)e];
-            count += w * (double)texels;
-        }
-    }
-    std::vector<double> mu((size_t)nout, 0.0), cov((size_t)nout * nout, 0.0);
-    for (int r = 0; r < nout; r++)
-        mu[(size_t)r] = count > 0.0 ? raw[(size_t)r] / count : 0.0;
-    for (int r = 0; r < nout; r++)
-        for (int s = 0; s < nout; s++)
-            cov[(size_t)r * nout + s] =
-                (count > 0.0 ? raw[(size_t)(nout + r * nout + s)] / count : 0.0) - mu[(size_t)r] * mu[(size_t)s];
-    for (int r = 0; r < nout; r++)
-        rep->total_variance += cov[(size_t)r * nout + r];
-    std::vector<double> u((size_t)nout, 0.0);
-    if (m->init0_texture)
-    {
-        int best = 0;
-        double best_value = -1.0;
-        std::vector<double> best_vec(3, 0.0);
-        for (int t = 0; t < m->textures; t++)
-        {
-            std::vector<double> block(9, 0.0);
-            for (int r = 0; r < 3; r++)
-                for (int s = 0; s < 3; s++)
-                    block[(size_t)r * 3 + s] = cov[(size_t)(3 * t + r) * nout + (3 * t + s)];
-            std::vector<double> work = block, vec, val;
-            jacobi_eigen(work, 3, vec, val);
-            int top = 0;
-            for (int i = 1; i < 3; i++)
-                if (val[(size_t)i] > val[(size_t)top])
-                    top = i;
-            if (val[(size_t)top] > best_value)
-            {
-                best_value = val[(size_t)top];
-                best = t;
-                for (int r = 0; r < 3; r++)
-                    best_vec[(size_t)r] = vec[(size_t)r * 3 + top];
-            }
-        }
-        rep->texture = best;
-        rep->eigenvalue = best_value > 0.0 ? best_value : 0.0;
-        for (int r = 0; r < 3; r++)
-            u[(size_t)(3 * best + r)] = best_vec[(size_t)r];
-    }
-    else
-    {
-        std::vector<double> work = cov, vec, val;
-        jacobi_eigen(work, nout, vec, val);
-        int top = 0;
-        for (int i = 1; i < nout; i++)
-            if (val[(size_t)i] > val[(size_t)top])
-                top = i;
-        rep->eigenvalue = val[(size_t)top];
-        for (int r = 0; r < nout; r++)
-            u[(size_t)r] = vec[(size_t)r * nout + top];
-    }
-    rep->share = rep->total_variance > 0.0 ? rep->eigenvalue / rep->total_variance : 0.0;
-    ProjDir dir{};
-    for (int r = 0; r < nout; r++)
-    {
-        dir.e[r] = u[(size_t)r];
-        dir.mu[r] = mu[(size_t)r];
-    }
-    int biggest = 0;
-    for (int r = 1; r < nout; r++)
-        if (std::fabs(dir.e[r]) > std::fabs(dir.e[biggest]))
-            biggest = r;
-    if (dir.e[biggest] < 0.0)
-        for (int r = 0; r < nout; r++)
-            dir.e[r] = -dir.e[r];
-    for (int r = 0; r < nout && r < MAX_NOUT; r++)
-        rep->dir[r] = dir.e[r];
-
-    double peak = 0.0;
-    std::vector<double> partial((size_t)COV_GRID, 0.0);
-    for (size_t i = 0; i < d->planes.size(); i++)
+    int used = 0;
+    const size_t scope = m->init0_chain ? d->planes.size() : 1;
+    for (size_t i = 0; i < scope; i++)
     {
         const DevPlane& p = d->planes[i];
+        const double w = m->init0_chain ? plane_weight[i] : 1.0;
+        if (!(w > 0.0))
+            continue;
         const size_t texels = (size_t)p.w0 * p.h0;
-        NB_TRY(residual_pass(d, i));
-        k_proj_peak<<<COV_GRID, 256, 0, d->stream>>>(d->resid, texels, nout, dir, d->cov);
+        k_moments<ResidualRows><<<COV_GRID, 256, 0, d->stream>>>(residual_rows(d, p), texels, nout, w, used ? 1 : 0,
+                                                                 d->cov);
         NB_LAUNCHED();
-        NB_TRY(download(d, partial.data(), d->cov, partial.size() * sizeof(double)));
-        for (int b = 0; b < COV_GRID; b++)
-            peak = std::max(peak, partial[(size_t)b]);
+        count += w * (double)texels;
+        used++;
     }
-    rep->peak = peak;
-    rep->divisor = peak;
-    double divisor = peak;
-    const int BINS = HIST_BINS;
-    if (!m->l0_bc8 && peak > 0.0)
+    if (!used)
+        NB_CUDA(cudaMemsetAsync(d->cov, 0, (size_t)MOM_ENTRIES * COV_GRID * sizeof(double), d->stream));
+    BasisArgs a{};
+    a.nout = nout;
+    a.mode = m->init0_texture ? 2 : 1;
+    a.components = 1;
+    a.textures = m->textures;
+    a.count = count;
+    Basis* B = reinterpret_cast<Basis*>(d->basis);
+    k_basis<<<1, 256, 0, d->stream>>>(d->cov, a, B);
+    NB_LAUNCHED();
+    // the projection's peak, the percentile (palette), then the seed, every plane of the chain
+    ResidualPassArgs ra{};
+    ra.channel = channel;
+    ra.levels = m->l0_bc8 ? 255 : (1 << m->bits0[channel]) - 1;
+    ra.palette_mode = m->l0_bc8 ? 0 : 1;
+    ra.palette = d->palette;
+    ra.hist = d->hist;
+    unsigned long long total = 0ull;
+    for (const DevPlane& p : d->planes)
     {
-        NB_CUDA(cudaMemsetAsync(d->hist, 0, BINS * sizeof(unsigned long long), d->stream));
-        unsigned long long total = 0ull;
-        for (size_t i = 0; i < d->planes.size(); i++)
-        {
-            const DevPlane& p = d->planes[i];
-            const size_t texels = (size_t)p.w0 * p.h0;
-            NB_TRY(residual_pass(d, i));
-            k_proj_hist<<<COV_GRID, 256, 0, d->stream>>>(d->resid, texels, nout, dir, 1.0 / peak, BINS, d->hist);
-            NB_LAUNCHED();
-            total += (unsigned long long)texels;
-        }
-        std::vector<unsigned long long> hist((size_t)BINS);
-        NB_TRY(download(d, hist.data(), d->hist, hist.size() * sizeof(unsigned long long)));
-        const unsigned long long want = (unsigned long long)(0.99 * (double)total);
-        unsigned long long cum = 0ull;
-        int bin = BINS - 1;
-        for (int b = 0; b < BINS; b++)
-        {
-            cum += hist[(size_t)b];
-            if (cum >= want)
-            {
-                bin = b;
-                break;
-            }
-        }
-        divisor = peak * (double)(bin + 1) / (double)BINS;
-        if (!(divisor > 0.0))
-            divisor = peak;
-        rep->divisor = divisor;
+        const size_t texels = (size_t)p.w0 * p.h0;
+        k_residual_pass<RP_PEAK><<<grid_for(texels, 256), 256, 0, d->stream>>>(residual_rows(d, p), texels, B, ra);
+        NB_LAUNCHED();
+        total += texels;
     }
-    const double inv = divisor > 0.0 ? 1.0 / divisor : 0.0;
-    const int levels = m->l0_bc8 ? 255 : (1 << m->bits0[channel]) - 1;
+    if (!m->l0_bc8)
+    {
+        NB_CUDA(cudaMemsetAsync(d->hist, 0, HIST_BINS * sizeof(unsigned long long), d->stream));
+        for (const DevPlane& p : d->planes)
+        {
+            const size_t texels = (size_t)p.w0 * p.h0;
+            k_residual_pass<RP_HIST><<<grid_for(texels, 256), 256, 0, d->stream>>>(residual_rows(d, p), texels, B,
+                                                                                     ra);
+            NB_LAUNCHED();
+        }
+    }
+    k_divisor<<<1, 256, 0, d->stream>>>(B, d->hist, total, m->l0_bc8 ? 0 : 1);
+    NB_LAUNCHED();
     for (size_t i = 0; i < d->planes.size(); i++)
     {
         const DevPlane& p = d->planes[i];
         const size_t texels = (size_t)p.w0 * p.h0;
-        NB_TRY(residual_pass(d, i));
-        k_seed_channel<<<grid_for(texels, 256), 256, 0, d->stream>>>(d->resid, texels, nout, dir, inv, d->c0, channel,
-                                                                     levels, d->palette, m->l0_bc8 ? 0 : 1, p.v0,
-                                                                     p.k0);
+        k_residual_pass<RP_SEED><<<grid_for(texels, 256), 256, 0, d->stream>>>(residual_rows(d, p), texels, B, ra);
         NB_LAUNCHED();
         if (!m->l0_bc8 && k0_io && k0_io[i])
-            NB_TRY(download(d, k0_io[i], p.k0, texels * d->c0));
+            NB_CUDA(cudaMemcpyAsync(k0_io[i], p.k0, texels * d->c0, cudaMemcpyDeviceToHost, d->stream));
     }
-    NB_CUDA(cudaStreamSynchronize(d->stream));
+    Basis h;
+    NB_TRY(download(d, &h, B, sizeof(h)));
+    rep->eigenvalue = h.eig[0];
+    rep->total_variance = h.total_variance;
+    rep->share = h.total_variance > 0.0 ? h.eig[0] / h.total_variance : 0.0;
+    std::memcpy(&rep->peak, &h.peak_bits[0], sizeof(double));
+    rep->divisor = h.divisor;
+    rep->texture = h.texture;
+    for (int r = 0; r < nout; r++)
+        rep->dir[r] = h.dir[0][r];
     return NNTC_B200_OK;
 }
 
 int nntc_b200_quantise_level1(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k1_out)
 {
-    const std::vector<std::vector<float>> on_device;
-    return fit_and_snap(d, m, 0, on_device, range_pct != 0, k1_out, true);
+    return fit_and_snap(d, m, 0, range_pct != 0, k1_out, true);
 }
 
 int nntc_b200_freeze_level1_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k1_out)
 {
-    const std::vector<std::vector<float>> on_device;
-    return fit_and_snap(d, m, 0, on_device, range_pct != 0, k1_out, true);
+    return fit_and_snap(d, m, 0, range_pct != 0, k1_out, true);
 }
 
-static int level0_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out)
+static int level0_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out, bool fit)
 {
     if (!d->l0_bc8)
     {
         set_error(NNTC_B200_ERR_STATE, "level 0 has a grid only under --l0 bc8");
         return NNTC_B200_ERR_STATE;
     }
-    const std::vector<std::vector<float>> on_device;
-    return fit_and_snap(d, m, 1, on_device, range_pct != 0, k0_out, true);
+    return fit_and_snap(d, m, 1, range_pct != 0, k0_out, fit);
 }
 
 int nntc_b200_quantise_level0(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out)
 {
-    return level0_grid(d, m, range_pct, k0_out);
+    return level0_grid(d, m, range_pct, k0_out, true);
 }
 
 int nntc_b200_freeze_level0_grid(nntc_b200_device* d, nntc_b200_model* m, int range_pct, uint8_t* const* k0_out)
 {
-    return level0_grid(d, m, range_pct, k0_out);
+    return level0_grid(d, m, range_pct, k0_out, true);
 }
 
 int nntc_b200_snap_level0_on_grid(nntc_b200_device* d, const nntc_b200_model* m, uint8_t* const* k0_out)
 {
-    if (!d->l0_bc8)
-    {
-        set_error(NNTC_B200_ERR_STATE, "level 0 has a grid only under --l0 bc8");
-        return NNTC_B200_ERR_STATE;
-    }
     nntc_b200_model copy = *m;
-    std::vector<std::vector<float>> none;
-    return fit_and_snap(d, &copy, 1, none, false, k0_out, false);
+    return level0_grid(d, &copy, 0, k0_out, false);
 }
 
 }   // extern "C"

@@ -696,7 +696,7 @@ __global__ void __launch_bounds__(THREADS) k_cg_update(Planes P, Red R)
 
 // beta, the residual, and the device-side stop: at an iteration that is a multiple of CG_PROBE a plane whose residual
 // is not at or above the tolerance leaves (the reference's host probe, src/solve_level1.cu:1288-1302).
-__global__ void k_cg_beta(Planes P, Red R, int it, unsigned int* active_count)
+__global__ void k_cg_beta(Planes P, Red R, int it, unsigned int* active_count, double tol)
 {
     const int pl = blockIdx.x;
     double* s = R.scalars + (size_t)pl * S_COUNT;
@@ -715,7 +715,7 @@ __global__ void k_cg_beta(Planes P, Red R, int it, unsigned int* active_count)
         const double rhs2 = s[S_RHS2];
         s[S_RESID] = rhs2 > 0.0 ? sqrt((rr > 0.0 ? rr : 0.0) / rhs2) : 0.0;
         s[S_ITER] = (double)(it + 1);
-        if ((it + 1) % CG_PROBE == 0 && !(s[S_RESID] >= CG_TOL))
+        if ((it + 1) % CG_PROBE == 0 && !(s[S_RESID] >= tol))
             s[S_ACTIVE] = 0.5;   // leaves after this iteration's direction update (which no longer matters)
         else
             atomicAdd(active_count, 1u);
@@ -974,9 +974,13 @@ static Red red_for(nntc_b200_device* d, const Planes& P)
     return Red{ d->partial, (size_t)(P.start[P.n] / THREADS), d->scalars };
 }
 
-int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono);
+int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono,
+                   int slots);
+int matvec_free(nntc_b200_device* d, const Planes& P, double* partial, int level0);
 
-int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0)
+// diag_only: the gradient and the diagonal blocks (slot 0) alone, what the matrix-free conjugate gradients of the
+// adjoint form need (their products come from adjoint_cg.cu, not from the other four slots).
+int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0, bool diag_only = false)
 {
     if (level0 && !d->l0_bc8)
     {
@@ -992,8 +996,8 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
     const size_t shared = (size_t)SLOTS * nmono * ASM_THREADS * sizeof(double);
     AsmArgs A{ d->weights, d->bias, d->cw, d->mono[level0], nmono };
     NB_TRY(ktimer_begin(d, level0 ? NNTC_B200_K_ASSEMBLE0 : NNTC_B200_K_ASSEMBLE1));
-    if (!d->reference_shaped_assembly && k <= 4)
-        NB_TRY(assemble_split(d, k, level0, P, nmono, mono.data()));
+    if (diag_only || (!d->reference_shaped_assembly && k <= 4))
+        NB_TRY(assemble_split(d, k, level0, P, nmono, mono.data(), diag_only ? 1 : SLOTS));
     else if (level0)
     {
         NB_CUDA(cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
@@ -1005,7 +1009,7 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
         k_assemble<false><<<blocks, ASM_THREADS, shared, d->stream>>>(P, A);
     }
     NB_TRY(ktimer_end(d));
-    if (d->reference_shaped_assembly || k > 4)
+    if (!diag_only && (d->reference_shaped_assembly || k > 4))
         NB_LAUNCHED();
     const Red R = red_for(d, P);
     const int tblocks = (int)(P.start[P.n] / THREADS);
@@ -1040,8 +1044,10 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     const int nc = level0 ? d->c0 : d->c1;
     for (int i = 0; i < np; i++)
         rep[i] = nntc_b200_plane_report{};
+    // the adjoint form: the gradient and the diagonal blocks assembled, the products matrix-free (adjoint_cg.cu)
+    const bool adjoint = d->adjoint_cg != 0 && k <= 4;
     NB_TRY(block_begin(d));
-    NB_TRY(assemble(d, m, k, ridge, level0));
+    NB_TRY(assemble(d, m, k, ridge, level0, adjoint));
     NB_CUDA(cudaEventRecord(d->ev[2], d->stream));
     Planes P = texel_planes(d, level0, k);
     const Red R = red_for(d, P);
@@ -1055,16 +1061,21 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     for (int it = 0; it < CG_MAX_IT; it++)
     {
         NB_CUDA(cudaMemsetAsync(active + (it % CG_PROBE), 0, sizeof(unsigned int), d->stream));
-        NB_TRY(ktimer_begin(d, NNTC_B200_K_MATVEC));
-        switch (P.c)
+        NB_TRY(ktimer_begin(d, level0 ? NNTC_B200_K_MATVEC0 : NNTC_B200_K_MATVEC));
+        if (adjoint)
+            NB_TRY(matvec_free(d, P, R.partial, level0));
+        else
         {
-        case 1: k_cg_matvec<1><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
-        case 2: k_cg_matvec<2><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
-        case 3: k_cg_matvec<3><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
-        default: k_cg_matvec<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+            switch (P.c)
+            {
+            case 1: k_cg_matvec<1><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+            case 2: k_cg_matvec<2><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+            case 3: k_cg_matvec<3><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+            default: k_cg_matvec<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+            }
+            NB_LAUNCHED();
         }
         NB_TRY(ktimer_end(d));
-        NB_LAUNCHED();
         k_cg_alpha<<<P.n, 32, 0, d->stream>>>(P, R);
         NB_LAUNCHED();
         switch (P.c)
@@ -1075,7 +1086,7 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
         default: k_cg_update<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
         }
         NB_LAUNCHED();
-        k_cg_beta<<<P.n, 32, 0, d->stream>>>(P, R, it, active + (it % CG_PROBE));
+        k_cg_beta<<<P.n, 32, 0, d->stream>>>(P, R, it, active + (it % CG_PROBE), adjoint ? CG_TOL_FP32 : CG_TOL);
         NB_LAUNCHED();
         k_cg_direction<<<tblocks, THREADS, 0, d->stream>>>(P, R);
         NB_LAUNCHED();
@@ -1128,8 +1139,10 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     const int nc = level0 ? d->c0 : d->c1;
     for (int i = 0; i < np; i++)
         rep[i] = nntc_b200_plane_report{};
+    // the adjoint form: the gradient and the diagonal blocks assembled, the products matrix-free (adjoint_cg.cu)
+    const bool adjoint = d->adjoint_cg != 0 && k <= 4;
     NB_TRY(block_begin(d));
-    NB_TRY(assemble(d, m, k, ridge, level0));
+    NB_TRY(assemble(d, m, k, ridge, level0, adjoint));
     NB_CUDA(cudaEventRecord(d->ev[2], d->stream));
     Planes P = texel_planes(d, level0, k);
     k_snapshot<<<(int)(P.start[P.n] / THREADS), THREADS, 0, d->stream>>>(P);
@@ -1213,6 +1226,16 @@ int nntc_b200_set_option(nntc_b200_device* d, int option, int value)
     if (option == NNTC_B200_OPT_REFERENCE_SHAPED_ASSEMBLY)
     {
         d->reference_shaped_assembly = value != 0;
+        return NNTC_B200_OK;
+    }
+    if (option == NNTC_B200_OPT_MIXED_PRECISION_GRAM)
+    {
+        d->mixed_gram = value != 0;
+        return NNTC_B200_OK;
+    }
+    if (option == NNTC_B200_OPT_ADJOINT_CG)
+    {
+        d->adjoint_cg = value != 0;
         return NNTC_B200_OK;
     }
     set_error(NNTC_B200_ERR_ARG, "no such option");

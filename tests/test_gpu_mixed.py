@@ -1,0 +1,56 @@
+"""The mixed-precision decoder fit on a B200: block (a)'s normal equations on the tcgen05 tensor cores (BF16 hi + lo
+split site rows, FP32 accumulators in tensor memory, FP64 across batches of 256 sites) against the same sums formed
+exactly (products of floats are exact in double, summed in FP64), on the same state.
+
+Bars: every entry of the system within 2e-6 of the largest entry of its kind (the split holds each factor to about
+2^-17 of itself); the decoder the device Cholesky solves from it within 1e-4 relative of the FP64 form's decoder
+(relative to the largest coefficient of the same output row), which is the bar the mixed-precision form is held to
+against the FP64 oracle; and the tensor-core sums are the same bits on a second run (fixed-order reduction)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from nntc_b200 import abi, check, lib, materials
+from nntc_b200.session import Session
+
+pytestmark = pytest.mark.gpu
+
+
+def state(seed, w, h, textures, c0, c1, k=4):
+    mat = materials.small(seed, w, h, textures=textures, c0=c0, c1=c1, k=k)
+    rng = np.random.default_rng(seed)
+    v0 = [(rng.random(p[0] * p[1] * c0) * 2 - 1).astype(np.float32) for p in mat.planes]
+    v1 = [(rng.random(p[2] * p[3] * c1) * 2 - 1).astype(np.float32) for p in mat.planes]
+    return mat, v0, v1
+
+
+def solve(s, mixed, k):
+    check(lib().nntc_b200_set_option(s.d, abi.OPT_MIXED_PRECISION_GRAM, 1 if mixed else 0), "option")
+    s.m.has_decoder = 0
+    s.solve_decoder(k)
+    w, b = s.decoder()
+    return s.normal_equations(), np.concatenate([w.reshape(s.m.nout, -1), b.reshape(-1, 1)], axis=1)
+
+
+@pytest.mark.parametrize("textures,c0,c1,w,h,k", [(4, 4, 4, 128, 96, 4), (6, 4, 4, 70, 52, 4), (1, 2, 4, 64, 64, 4),
+                                                  (2, 3, 2, 45, 31, 2), (3, 1, 1, 33, 20, 0)])
+def test_tensor_core_normal_equations_vs_fp64(textures, c0, c1, w, h, k):
+    mat, v0, v1 = state(w * h + textures, w, h, textures, c0, c1, k)
+    with Session(mat) as s:
+        for i in range(len(mat.planes)):
+            s.set_planes(i, v0[i], v1[i])
+        s.set_grids(np.full(c0, -1.0), np.full(c0, 1.0))
+        ne64, x64 = solve(s, False, k)
+        ne_tc, x_tc = solve(s, True, k)
+        ne_tc2, _ = solve(s, True, k)
+    mm = abi.feature_count(c0, c1) + 1
+    tri = mm * (mm + 1) // 2
+    for part in (slice(0, tri), slice(tri, ne64.size)):
+        scale = np.abs(ne64[part]).max()
+        err = np.abs(ne_tc[part] - ne64[part]).max()
+        assert err <= 2e-6 * scale, (err / scale)
+    assert np.array_equal(ne_tc, ne_tc2), "the tensor-core sums are not reproducible"
+    row_scale = np.abs(x64).max(axis=1, keepdims=True)
+    rel = np.abs(x_tc - x64) / row_scale
+    assert rel.max() <= 1e-4, rel.max()
