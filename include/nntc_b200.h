@@ -271,6 +271,12 @@ typedef struct nntc_b200_encode_args
     int bc_refine_after;   /* --bc-refine-after 0 */
     int bc_outer;          /* --bc-outer 2 */
     float luma[3];         /* 0.299, 0.587, 0.114 */
+    /* 0: the plain form, the reference's arithmetic (FP64 stencils and sums). 1: the adjoint + mixed-precision form:
+     * block (a)'s sums on the tensor cores (NNTC_B200_OPT_MIXED_PRECISION_GRAM), the conjugate gradients matrix-free
+     * in FP32 (NNTC_B200_OPT_ADJOINT_CG), and after the repack passes one joint latent / decoder pass (bc8): a step
+     * of both latents along their preconditioned objective gradient with the decoder re-solved, the best of three
+     * step lengths, re-packed and refined, kept only when the shipped E falls. Has no counterpart in the reference. */
+    int form;
 } nntc_b200_encode_args;
 
 typedef struct nntc_b200_encode_result
@@ -283,6 +289,9 @@ typedef struct nntc_b200_encode_result
     double psnr[6];        /* per texture: 8-bit decode at the base plane's texel centres vs the source bytes */
     double ms_a, ms_b, ms_c, ms_e, ms_pack, ms_refine, ms_total;   /* CUDA-event spans of each kind of block */
     long long objective_passes;
+    int joint_taken;       /* form 1: the joint pass was kept (the shipped E fell) */
+    double e_joint;        /* form 1: the shipped E the joint pass reached, kept or not (0 when it did not run) */
+    double ms_joint;       /* form 1: the joint pass's span */
 } nntc_b200_encode_result;
 
 void nntc_b200_encode_defaults(nntc_b200_encode_args* a);
@@ -292,6 +301,15 @@ void nntc_b200_encode_defaults(nntc_b200_encode_args* a);
 int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_args* a,
                                const double* per_site, nntc_b200_encode_result* r, uint8_t* const* k0,
                                uint8_t* const* k1, uint8_t* const* ep, uint8_t* const* sel);
+
+/* The gradient of the objective E (the normalised E of nntc_b200_objective_eval) at the current state, with respect to
+ * every level-1 value (g_v1[i]: w1 h1 c1 doubles per plane), every level-0 value (g_v0[i]: w0 h0 c0 doubles per
+ * plane; bc8 only, else pass null) and the decoder (g_dec: nout rows of [dE/dW_c (nin) | dE/db_c]), from one pass of
+ * the decode's adjoint: the latents' parts are the assembly's J^T diag(cw) r gathered per texel, the decoder's part
+ * 2 cw_c (A x_c - rhs_c) from the normal equations at the current latents. No counterpart in the reference (its
+ * gradients live inside its stencil assembly and are not exposed). */
+int nntc_b200_objective_gradient(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                                 double* const* g_v0, double* const* g_v1, double* g_dec);
 
 /* ---- kernel-shape options: the results are the same bits either way ---- */
 enum nntc_b200_option

@@ -25,6 +25,7 @@ _PD = C.POINTER(C.c_double)
 _PU8 = C.POINTER(C.c_uint8)
 _PPF = C.POINTER(_PF)
 _PPU8 = C.POINTER(_PU8)
+_PPD = C.POINTER(_PD)
 _M = C.POINTER(abi.Model)
 
 PROTOTYPES = {
@@ -82,6 +83,7 @@ PROTOTYPES = {
     "nntc_b200_encode_on_device": (_I, [_P, _M, C.POINTER(abi.EncodeArgs), _PD, C.POINTER(abi.EncodeResult),
                                         _PPU8, _PPU8, _PPU8, _PPU8]),
     "nntc_b200_set_option": (_I, [_P, _I, _I]),
+    "nntc_b200_objective_gradient": (_I, [_P, _M, _I, _PD, _PPD, _PPD, _PD]),
     "nntc_b200_probe_normal_equations": (_I, [_P, _PD, _S]),
     "nntc_b200_probe_workspace": (_I, [_P, _I, _I, _PD, _PD, _PF, _PD, _PF]),
     "nntc_b200_probe_monomials": (_I, [_P, _I, _PD, _S]),

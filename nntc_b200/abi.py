@@ -74,7 +74,7 @@ class EncodeArgs(C.Structure):
     _fields_ = [("k", C.c_int), ("rounds", C.c_int), ("tol", C.c_double), ("q1_start", C.c_int),
                 ("q1_sweeps", C.c_int), ("range_pct", C.c_int), ("ridge", C.c_double), ("sweeps", C.c_int),
                 ("init_pca", C.c_int), ("bc_refine", C.c_int), ("bc_refine_after", C.c_int), ("bc_outer", C.c_int),
-                ("luma", C.c_float * 3)]
+                ("luma", C.c_float * 3), ("form", C.c_int)]
 
 
 class EncodeResult(C.Structure):
@@ -82,7 +82,8 @@ class EncodeResult(C.Structure):
                 ("e_after_rounds", C.c_double), ("e_ship", C.c_double), ("centre_mse", C.c_double),
                 ("sampled_mse", C.c_double), ("psnr", C.c_double * 6), ("ms_a", C.c_double), ("ms_b", C.c_double),
                 ("ms_c", C.c_double), ("ms_e", C.c_double), ("ms_pack", C.c_double), ("ms_refine", C.c_double),
-                ("ms_total", C.c_double), ("objective_passes", C.c_longlong)]
+                ("ms_total", C.c_double), ("objective_passes", C.c_longlong), ("joint_taken", C.c_int),
+                ("e_joint", C.c_double), ("ms_joint", C.c_double)]
 
 
 # nntc_b200_set_option's options (include/nntc_b200.h, enum nntc_b200_option)

@@ -53,6 +53,94 @@ int snapshot(nntc_b200_device* d, bool save)
 
 namespace nb
 {
+int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0);
+int joint_apply(nntc_b200_device* d, const nntc_b200_model* m, int k, int level0, float alpha);
+}
+
+namespace
+{
+
+// The adjoint form's joint pass (bc8, after the repack passes; the method is described in joint.cu): both latents step
+// along their preconditioned objective gradients by the best of alpha in {1, 1/2, 1/4} (snapped onto their grids, the
+// decoder re-solved at every trial), the step is re-packed into BC blocks and refined, and the whole pass is kept only
+// when the shipped E falls below e_ship; otherwise every part of the state is restored exactly.
+template <class Obj, class BlockA>
+int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_args* a, int k,
+               const double* per_site, Obj objective, BlockA block_a, double& e_ship, nntc_b200_encode_result* r)
+{
+    (void)per_site;
+    cudaEvent_t j0, j1;
+    NB_CUDA(cudaEventCreate(&j0));
+    NB_CUDA(cudaEventCreate(&j1));
+    NB_CUDA(cudaEventRecord(j0, d->stream));
+    NB_TRY(snapshot(d, true));
+    const nntc_b200_model keep_m = *m;
+    auto restore = [&]() -> int {
+        NB_TRY(snapshot(d, false));
+        *m = keep_m;
+        NB_TRY(nntc_b200_upload_decoder(d, m));
+        return nntc_b200_upload_grids(d, m);
+    };
+    NB_TRY(nb::descent_direction(d, m, k, a->ridge, 0));
+    NB_TRY(nb::descent_direction(d, m, k, a->ridge, 1));
+    nntc_b200_objective e{};
+    NB_TRY(objective(e));
+    double best_e = e.e;
+    float best = 0.0f;
+    for (float alpha = 1.0f; alpha >= 0.25f; alpha *= 0.5f)
+    {
+        *m = keep_m;
+        NB_TRY(nntc_b200_upload_decoder(d, m));
+        NB_TRY(nb::joint_apply(d, m, k, 0, alpha));
+        NB_TRY(nb::joint_apply(d, m, k, 1, alpha));
+        NB_TRY(block_a());
+        NB_TRY(objective(e));
+        if (e.e < best_e)
+        {
+            best_e = e.e;
+            best = alpha;
+        }
+    }
+    int st = NNTC_B200_OK;
+    if (best == 0.0f)
+        st = restore();
+    else
+    {
+        *m = keep_m;
+        NB_TRY(nntc_b200_upload_decoder(d, m));
+        NB_TRY(nb::joint_apply(d, m, k, 0, best));
+        NB_TRY(nb::joint_apply(d, m, k, 1, best));
+        NB_TRY(block_a());
+        double ms = 0.0;
+        NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, nullptr, &ms));
+        r->ms_pack += ms;
+        std::vector<nntc_b200_bc_report> rp((size_t)(a->bc_refine > 0 ? a->bc_refine : 1));
+        NB_TRY(nntc_b200_bc_refine(d, m, a->bc_refine, rp.data(), &ms));
+        r->ms_refine += ms;
+        NB_TRY(objective(e));
+        r->e_joint = e.e;
+        if (e.e < e_ship)
+        {
+            e_ship = e.e;
+            r->joint_taken = 1;
+        }
+        else
+            st = restore();
+    }
+    NB_CUDA(cudaEventRecord(j1, d->stream));
+    NB_CUDA(cudaEventSynchronize(j1));
+    float jm = 0.0f;
+    NB_CUDA(cudaEventElapsedTime(&jm, j0, j1));
+    r->ms_joint = jm;
+    cudaEventDestroy(j0);
+    cudaEventDestroy(j1);
+    return st;
+}
+
+}   // namespace
+
+namespace nb
+{
 int channel_copies(nntc_b200_device* d, std::vector<unsigned char>& same);
 int psnr_base(nntc_b200_device* d, const nntc_b200_model* m, double* psnr);
 }
@@ -89,6 +177,28 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     *r = nntc_b200_encode_result{};
     const int np = m->nplanes, k = a->k;
     const bool bc8 = m->l0_bc8 != 0;
+    // The adjoint + mixed-precision form: the tensor-core normal equations and the matrix-free conjugate gradients for
+    // this encode, the device's own settings put back on every way out.
+    struct FormScope
+    {
+        nntc_b200_device* d;
+        int gram, cg;
+        ~FormScope()
+        {
+            d->mixed_gram = gram;
+            d->adjoint_cg = cg;
+        }
+    } form_scope{ d, d->mixed_gram, d->adjoint_cg };
+    if (a->form == 1)
+    {
+        d->mixed_gram = 1;
+        d->adjoint_cg = 1;
+    }
+    else if (a->form != 0)
+    {
+        set_error(NNTC_B200_ERR_ARG, "form must be 0 (plain) or 1 (adjoint + mixed precision)");
+        return NNTC_B200_ERR_ARG;
+    }
     cudaEvent_t t0, t1;
     NB_CUDA(cudaEventCreate(&t0));
     NB_CUDA(cudaEventCreate(&t1));
@@ -373,6 +483,8 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             NB_TRY(nntc_b200_upload_grids(d, m));
             break;
         }
+        if (a->form == 1)
+            NB_TRY(joint_pass(d, m, a, k, per_site, objective, block_a, e_ship, r));
         NB_TRY(refit_level1());
         NB_TRY(block_a());
     }

@@ -1204,6 +1204,21 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
 }
 
 // Block (c')'s assembly alone with no ridge, the correction measured from the plane as it stands (for refine_bc).
+// The gradient, the diagonal blocks and the preconditioned descent direction of one latent at its current plane:
+// grad, z = -(H_tt + lambda I)^-1 grad texel by texel, prev = v (what the joint pass steps from).
+int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0)
+{
+    NB_TRY(assemble(d, m, k, ridge, level0, true));
+    Planes P = texel_planes(d, level0, k);
+    const Red R = red_for(d, P);
+    const int tblocks = (int)(P.start[P.n] / THREADS);
+    k_precondition_init<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    NB_LAUNCHED();
+    k_snapshot<<<tblocks, THREADS, 0, d->stream>>>(P);
+    NB_LAUNCHED();
+    return NNTC_B200_OK;
+}
+
 int assemble_for_refine(nntc_b200_device* d, const nntc_b200_model* m, int k, double* ms)
 {
     NB_TRY(block_begin(d));
