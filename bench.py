@@ -1,22 +1,27 @@
 """Encode throughput of the B200 NNTC encoder hot path: one step = one whole encode of the workload material.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form adjoint|plain] [--config C]
 
 Metric: encode Mpix/s = base W x H of the material / encode seconds (the reference's `time ... s total` definition,
-src/main.cpp:1788-2948, with the base extent). N > 1 runs under torchrun as REPLICAS: every rank encodes its own
-seeded material of the same configuration on its own GPU, with no collective on the data path (the encode does not
-shard; one material per GPU); the whole-job value is the pixels of every rank over the slowest rank's time.
+src/main.cpp:1788-2948, with the base extent), for the adjoint + mixed-precision form against the plain form on the
+same GPU. N > 1 runs under torchrun as REPLICAS: every rank encodes its own seeded material of the same configuration
+on its own GPU, with no collective on the data path (the encode does not shard; one material per GPU); the whole-job
+value is the pixels of every rank over the slowest rank's time.
 
-- `value`: the encode on a device model whose source chain is already resident in HBM, timed by the library's CUDA
-  events on its own stream around the whole encode (nntc_b200_encode_result.ms_total), K steps bracketed by a barrier
-  and a synchronize, max over ranks.
-- `e2e`: the same through the C ABI with host buffers: device_create_from_base (the base plane's H2D copy from pinned
-  host memory, the rest of the source chain built on the device), the encode, and the D2H read of its result (indices,
-  BC endpoints/selectors, decoder) every step.
+- `value`: the `--form` encode (default adjoint) on a device model whose source chain is already resident in HBM,
+  timed by the library's CUDA events on its own stream around the whole encode (nntc_b200_encode_result.ms_total), K
+  steps bracketed by a barrier and a synchronize, max over ranks. Every encode forms its own per-material caches.
+- `forms`: both forms on the same material and GPU - ms per encode, PSNR per texture, the adjoint / plain speed ratio,
+  the PSNR delta, and whether the adjoint form's joint pass was kept; the other form is timed over --compare-steps.
+- `e2e`: the `--form` encode through the C ABI with host buffers: device_create_from_base (the base plane's H2D copy
+  from pinned host memory, the rest of the source chain built on the device), the encode, the D2H read of its result
+  (indices, BC endpoints/selectors, decoder) and the asset written to disk, every step.
 - `roofline`: the dominant kernel's achieved rate from per-launch CUDA events over the timed steps
   (nntc_b200_kernel_stats), against MEASURED_PEAKS.json.
+- `reference_cuda`: the reference's own CUDA encoder (oracle/_ref/nntc_encode_cuda, its sources unmodified, compiled
+  for sm_100) on the same material on the same GPU, once: its own `time ... s total` and per-texture PSNR.
 - `cpu_baseline`: the reference's own CPU encoder (oracle/_ref/nntc_encode_cpu, built from the reference sources) on
-  a bounded crop of the same material, on this host's cores.
+  a bounded crop of the same material, on this host's cores, with this library's encode of the same crop beside it.
 - `--impl reference`: that reference CPU encoder alone, timed per step on the crop (rank 0; other ranks exit 0).
 The inputs are seeded synthetic textures with the shapes of the configuration (nntc_b200/materials.py); every step's
 working set is far larger than the 126 MB L2, so no flush is needed between steps.
@@ -170,15 +175,59 @@ def big_material(seed):
     return materials.config(4, seed=seed)
 
 
+KERNELS = ["objective", "normal_equations", "assemble_level1", "assemble_level0", "cg_product_level1",
+           "quant_sweep", "bc_refine", "cg_product_level0"]   # nntc_b200_kernel ids 0..7
+FORMS = {"plain": 0, "adjoint": 1}
+
+
+def encode_args(L, form):
+    ea = abi.EncodeArgs()
+    L.nntc_b200_encode_defaults(C.byref(ea))
+    ea.form = FORMS[form]
+    return ea
+
+
+def reference_cuda(mat, threads):
+    """The reference's own CUDA encoder (oracle/_ref/nntc_encode_cuda, its unmodified sources compiled for sm_100) on
+    the same material and layout, once: its `time ... s total` and per-texture PSNR."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "nntc_encode_cuda")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/nntc_encode_cuda is not built"}
+    tmp = tempfile.mkdtemp(prefix="nntc_refcuda_")
+    try:
+        pngs = materials.save_material(mat, os.path.join(tmp, "in"), level=1)
+        cmd = [exe, *pngs, "-o", os.path.join(tmp, "out") + "/", "--backend", "cuda", "--c0", str(mat.c0), "--c1",
+               str(mat.c1), "--png", "0", "-j", str(threads)]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        wall = time.perf_counter() - t0
+        if p.returncode != 0:
+            return {"unavailable": "the reference CUDA encoder failed: " + (p.stdout + p.stderr)[-300:]}
+        m = re.search(r"time\s+([\d.]+) s total", p.stdout)
+        secs = float(m.group(1)) if m else wall
+        psnr = [float(x) for x in re.findall(r"psnr\s+texture \d+\s+([\d.]+) dB", p.stdout)]
+        return {"value": round(mat.width * mat.height / 1e6 / secs, 6), "unit": "Mpix/s", "s_total": round(secs, 3),
+                "psnr": psnr, "span": "the reference's own time ... s total (PNG decode, encode, asset write)",
+                "build": "the reference's sources unmodified, kernels compiled for sm_100 with -fmad=false"}
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference CUDA encoder did not finish in 900 s"}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="adjoint", choices=["adjoint", "plain"],
+                    help="the form timed for `value` and `e2e`; the other form is timed beside it")
+    ap.add_argument("--compare-steps", type=int, default=3, help="timed encodes of the other form")
     ap.add_argument("--config", type=int, default=4)
     ap.add_argument("--crop", type=int, default=256, help="edge of the CPU-baseline crop")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -195,8 +244,6 @@ def main():
     mat = materials.config(args.config, seed=rank) if args.config != 4 else big_material(rank)
     model = abi.make_model(mat)
     L = lib()
-    ea = abi.EncodeArgs()
-    L.nntc_b200_encode_defaults(C.byref(ea))
     per_site = (C.c_double * len(mat.per_site))(*mat.per_site)
     # a pinned host copy of the base plane: what the e2e leg copies to the device every step (the rest of the source
     # chain is built on the device from it)
@@ -217,15 +264,23 @@ def main():
     handle = C.c_void_p()
     check(L.nntc_b200_device_create_from_base(C.byref(model), base_ptr, C.byref(handle)), "device_create_from_base")
 
-    def encode_resident():
+    def encode_resident(ea):
         r = abi.EncodeResult()
         m = abi.make_model(mat)
         check(L.nntc_b200_encode_on_device(handle, C.byref(m), C.byref(ea), per_site, C.byref(r), None, None, None,
                                            None), "encode")
         return r
 
+    headline, other = args.form, ("plain" if args.form == "adjoint" else "adjoint")
+    ea = encode_args(L, headline)
+    # the other form first, a few encodes, for the form ratio and the PSNR delta
+    ea_other = encode_args(L, other)
+    encode_resident(ea_other)
+    other_results = [encode_resident(ea_other) for _ in range(args.compare_steps)]
+    other_ms = statistics.median(r.ms_total for r in other_results)
+
     for _ in range(args.warmup):
-        encode_resident()
+        encode_resident(ea)
     check(L.nntc_b200_kernel_timing(handle, 1), "timing")
     check(L.nntc_b200_kernel_stats(handle, 0, None, None, 1), "reset")
     launches0 = L.nntc_b200_launch_count()
@@ -236,7 +291,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            results.append(encode_resident())
+            results.append(encode_resident(ea))
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         if world > 1:
@@ -244,18 +299,19 @@ def main():
     launches = L.nntc_b200_launch_count() - launches0
     device_ms = sum(r.ms_total for r in results)
     stats = {}
-    for kid, name in enumerate(["objective", "normal_equations", "assemble_level1", "assemble_level0", "cg_matvec",
-                                "quant_sweep", "bc_refine"]):
+    for kid, name in enumerate(KERNELS):
         n = C.c_longlong()
         ms = C.c_double()
         check(L.nntc_b200_kernel_stats(handle, kid, C.byref(n), C.byref(ms), 0), "stats")
         stats[name] = (n.value, ms.value)
     check(L.nntc_b200_kernel_timing(handle, 0), "timing")
 
-    # e2e: through the C ABI with host buffers, every step's H2D of the chain and D2H of the result included; the
-    # resident model is released first, and one untimed step warms the path up
+    # e2e: through the C ABI with host buffers, every step's H2D of the base plane, the encode, the D2H of the shipped
+    # state and the asset written to disk (the .dds files and the descriptor); the resident model is released first,
+    # and one untimed step warms the path up
     L.nntc_b200_device_destroy(handle)
     e2e_ms = []
+    asset_dir = tempfile.mkdtemp(prefix="nntc_asset_")
 
     def e2e_step():
         h = C.c_void_p()
@@ -266,6 +322,9 @@ def main():
         check(L.nntc_b200_encode_on_device(h, C.byref(m), C.byref(ea), per_site, C.byref(r), abi.u8_ptrs(k0),
                                            abi.u8_ptrs(k1), abi.u8_ptrs(ep), abi.u8_ptrs(sel)), "encode")
         L.nntc_b200_device_destroy(h)
+        check(L.nntc_b200_write_asset(C.byref(m), abi.u8_ptrs(k0), abi.u8_ptrs(k1), abi.u8_ptrs(ep), abi.u8_ptrs(sel),
+                                      mat.width, mat.height, os.path.join(asset_dir, "bench").encode(), None, None),
+              "write_asset")
 
     e2e_step()
     if world > 1:
@@ -278,6 +337,7 @@ def main():
         ev1.record()
         ev1.synchronize()
         e2e_ms.append(ev0.elapsed_time(ev1))
+    shutil.rmtree(asset_dir, ignore_errors=True)
 
     device_ms, e2e_total = slowest(world, [device_ms, sum(e2e_ms)], "cuda")
     mpix = mat.width * mat.height / 1e6
@@ -288,38 +348,88 @@ def main():
         hbm, tf, src = peaks()
         dom = max(stats, key=lambda k: stats[k][1])
         roof = roofline(dom, stats[dom], mat, hbm, tf, src)
+        nt = len(mat.textures)
+        psnr_h = [round(x, 3) for x in results[-1].psnr[:nt]]
+        psnr_o = [round(x, 3) for x in other_results[-1].psnr[:nt]]
+        head_ms = device_ms / args.steps
+        forms = {headline: {"ms_per_encode": round(head_ms, 2), "mpix_s": round(mpix / (head_ms / 1000), 6),
+                            "psnr": psnr_h, "e_ship": results[-1].e_ship},
+                 other: {"ms_per_encode": round(other_ms, 2), "mpix_s": round(mpix / (other_ms / 1000), 6),
+                         "psnr": psnr_o, "e_ship": other_results[-1].e_ship, "steps": args.compare_steps}}
+        adj = forms["adjoint"]
+        pln = forms["plain"]
+        forms["adjoint_over_plain"] = round(pln["ms_per_encode"] / adj["ms_per_encode"], 4)
+        forms["psnr_delta_db"] = [round(a - b, 3) for a, b in zip(adj["psnr"], pln["psnr"])]
+        adj_res = results[-1] if headline == "adjoint" else other_results[-1]
+        forms["joint_pass"] = {"taken": adj_res.joint_taken, "e_reached": adj_res.e_joint,
+                               "ms": round(adj_res.ms_joint, 2)}
         line = {
             "metric": "encode Mpix/s", "value": round(value, 6), "unit": "Mpix/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(device_ms / args.steps, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(head_ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3+f32+f64" if headline == "adjoint" else "f32+f64",
             "data": "synthetic (seeded, nntc_b200/materials.py)",
-            "config": {"workload": CONFIG_NAMES[args.config], "base": [mat.width, mat.height],
-                       "textures": len(mat.textures), "c0": mat.c0, "c1": mat.c1, "k": mat.k,
+            "config": {"workload": CONFIG_NAMES[args.config], "form": headline, "base": [mat.width, mat.height],
+                       "textures": nt, "c0": mat.c0, "c1": mat.c1, "k": mat.k,
                        "chain_pixels": mat.chain_pixels, "parallelism": f"replicas x{world}",
                        "l2": "working set > 126 MB L2 every step, no flush needed",
-                       "psnr": [round(x, 3) for x in results[-1].psnr[: len(mat.textures)]],
-                       "rounds": results[-1].rounds_used, "wall_s_per_step": round(wall / args.steps, 3),
+                       "caches": "the per-material target caches are re-formed inside every encode",
+                       "psnr": psnr_h, "rounds": results[-1].rounds_used,
+                       "wall_s_per_step": round(wall / args.steps, 3),
                        "phase_ms": {k: round(getattr(results[-1], "ms_" + k), 2) for k in
-                                    ("a", "b", "c", "e", "pack", "refine", "total")},
+                                    ("a", "b", "c", "e", "pack", "refine", "joint", "total")},
                        "kernel_ms": {k: [v[0], round(v[1], 2)] for k, v in stats.items()}},
+            "forms": forms,
             "e2e": {"value": round(e2e_value, 6), "unit": "Mpix/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h,
+                    "span": "base plane H2D from pinned memory, chain built on the device, encode, D2H of the shipped "
+                            "state, asset (.dds + JSON) written to disk"},
             "gpu_launches": launches,
             "roofline": roof,
             "clocks": clocks.summary(),
         }
+        if world == 1 and not args.no_reference_cuda:
+            line["reference_cuda"] = reference_cuda(mat, os.cpu_count() or 1)
+            if "psnr" in line["reference_cuda"]:
+                line["reference_cuda"]["psnr_delta_db"] = [round(a - b, 3) for a, b in
+                                                           zip(psnr_h, line["reference_cuda"]["psnr"])]
         if not args.no_cpu_baseline and world == 1:
             crop = crop_material(mat, args.crop)
             secs, err = reference_cpu(crop, 1, 0, os.cpu_count() or 1)
-            line["cpu_baseline"] = ({"unavailable": err} if err else {
-                "value": round(crop.width * crop.height / 1e6 / secs[0], 6), "unit": "Mpix/s",
-                "cores": os.cpu_count(), "kind": "reference",
-                "sample": f"{args.crop}x{args.crop} crop of the workload ({len(mat.textures)} textures, c0 {mat.c0} "
-                          f"c1 {mat.c1}), whole encode by the reference CPU encoder, one run"})
+            if err:
+                line["cpu_baseline"] = {"unavailable": err}
+            else:
+                # this library on the same crop, the like-for-like ratio's other side
+                with_crop = crop_gpu_mpix(L, crop, ea)
+                line["cpu_baseline"] = {
+                    "value": round(crop.width * crop.height / 1e6 / secs[0], 6), "unit": "Mpix/s",
+                    "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"{args.crop}x{args.crop} crop of the workload ({nt} textures, c0 {mat.c0} c1 {mat.c1}), "
+                              f"whole encode by the reference CPU encoder, one run",
+                    "same_crop_gpu_mpix_s": round(with_crop, 6)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def crop_gpu_mpix(L, crop, ea):
+    """This library's encode of the CPU baseline's crop (resident, median of three after one warm-up)."""
+    per_site = (C.c_double * len(crop.per_site))(*crop.per_site)
+    chain = [np.ascontiguousarray(c, np.float32).ravel() for c in crop.chain]
+    model = abi.make_model(crop)
+    h = C.c_void_p()
+    check(L.nntc_b200_device_create(C.byref(model), abi.float_ptrs(chain), C.byref(h)), "device_create")
+    ms = []
+    for i in range(4):
+        r = abi.EncodeResult()
+        m = abi.make_model(crop)
+        check(L.nntc_b200_encode_on_device(h, C.byref(m), C.byref(ea), per_site, C.byref(r), None, None, None, None),
+              "encode")
+        if i:
+            ms.append(r.ms_total)
+    L.nntc_b200_device_destroy(h)
+    return crop.width * crop.height / 1e6 / (statistics.median(ms) / 1000.0)
 
 
 # DRAM bytes (read + write) per launch of each timed kernel group, per level-0 pixel of the chain, from one ncu capture
@@ -336,10 +446,12 @@ BINDING = {
     "assemble_level0": "FP32/ALU issue (site terms) and FP64 issue plus stencil stores (gather); not HBM",
     "assemble_level1": "FP32/ALU issue (site terms) and L2 latency (gather); not HBM",
     "objective": "FP64 pipe (~50% of peak)",
-    "normal_equations": "FP64 tensor pipe and site staging",
+    "normal_equations": "site-row formation (FP32/ALU issue); the tensor pipe (tcgen05, adjoint form) or the FP64 "
+                        "tensor pipe (plain form) is not the bound",
     "bc_refine": "latency: the set-up's scattered stencil reads, then the ordered selector steps (four evaluated at once)",
     "quant_sweep": "HBM (level-0 colour launch ~79% of measured copy bandwidth)",
-    "cg_matvec": "HBM",
+    "cg_product_level0": "HBM (plain form, FP64 stencil) / FP32 issue (adjoint form, matrix-free)",
+    "cg_product_level1": "HBM (plain form, FP64 stencil) / FP32 issue (adjoint form, matrix-free)",
 }
 
 
@@ -371,8 +483,10 @@ def algorithmic_bytes(name, mat):
         return t0 * (4 * nout + 4 * c0) + t1 * (4 * c1 + 5 * c1 * c1 * 8 + 8 * c1)
     if name == "objective" or name == "normal_equations":
         return t0 * (4 * nout + 4 * c0) + t1 * 4 * c1
-    if name == "cg_matvec":   # the larger of the two unknowns' stencils: own 5 blocks + x in + y out
-        return max(t0 * (5 * c0 * c0 * 8 + 3 * 8 * c0), t1 * (5 * c1 * c1 * 8 + 3 * 8 * c1))
+    if name == "cg_product_level0":   # the stencil's 5 blocks + x in + y out per level-0 texel
+        return t0 * (5 * c0 * c0 * 8 + 3 * 8 * c0)
+    if name == "cg_product_level1":
+        return t1 * (5 * c1 * c1 * 8 + 3 * 8 * c1)
     if name == "quant_sweep":   # one colour: a quarter of the texels read their 9 blocks' worth
         return max(t0 * (5 * c0 * c0 * 8 + 2 * 8 * c0 + 9 * c0) // 4 * 4 // 4, t1 * (5 * c1 * c1 * 8) // 4)
     if name == "bc_refine":   # one colour: a quarter of the blocks read their stencil, grad, planes

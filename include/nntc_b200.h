@@ -273,7 +273,8 @@ typedef struct nntc_b200_encode_args
     float luma[3];         /* 0.299, 0.587, 0.114 */
     /* 0: the plain form, the reference's arithmetic (FP64 stencils and sums). 1: the adjoint + mixed-precision form:
      * block (a)'s sums on the tensor cores (NNTC_B200_OPT_MIXED_PRECISION_GRAM), the conjugate gradients matrix-free
-     * in FP32 (NNTC_B200_OPT_ADJOINT_CG), and after the repack passes one joint latent / decoder pass (bc8): a step
+     * in FP32 (NNTC_B200_OPT_ADJOINT_CG), the objective's decode in FP32 (NNTC_B200_OPT_MIXED_OBJECTIVE), and after
+     * the repack passes one joint latent / decoder pass (bc8): a step
      * of both latents along their preconditioned objective gradient with the decoder re-solved, the best of three
      * step lengths, re-packed and refined, kept only when the shipped E falls. Has no counterpart in the reference. */
     int form;
@@ -290,6 +291,7 @@ typedef struct nntc_b200_encode_result
     double ms_a, ms_b, ms_c, ms_e, ms_pack, ms_refine, ms_total;   /* CUDA-event spans of each kind of block */
     long long objective_passes;
     int joint_taken;       /* form 1: the joint pass was kept (the shipped E fell) */
+    double e_before_joint; /* form 1: the shipped E the joint pass started from (0 when it did not run) */
     double e_joint;        /* form 1: the shipped E the joint pass reached, kept or not (0 when it did not run) */
     double ms_joint;       /* form 1: the joint pass's span */
 } nntc_b200_encode_result;
@@ -326,7 +328,11 @@ enum nntc_b200_option
      * and its adjoint in FP32, with FP64 inner products and recurrences, and stop at 1e-6 of the right-hand side; only
      * the gradient and the diagonal blocks are assembled (the adjoint form; NOT the same bits). 0 (default): the
      * assembled FP64 stencil (src/solve_level1.cu:781-828, 1222-1338). The quantised sweeps assemble in full either way. */
-    NNTC_B200_OPT_ADJOINT_CG = 2
+    NNTC_B200_OPT_ADJOINT_CG = 2,
+    /* 1: the objective's per-site decode in FP32 (the assembly's float tap rule and float targets) with every
+     * residual's square summed in FP64 (the adjoint form; E to about 1e-7 relative). 0 (default): the decode in FP64 on
+     * the double u-space sampling rule (src/objective.cu:97-211). */
+    NNTC_B200_OPT_MIXED_OBJECTIVE = 3
 };
 int nntc_b200_set_option(nntc_b200_device* d, int option, int value);
 

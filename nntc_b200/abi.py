@@ -83,13 +83,14 @@ class EncodeResult(C.Structure):
                 ("sampled_mse", C.c_double), ("psnr", C.c_double * 6), ("ms_a", C.c_double), ("ms_b", C.c_double),
                 ("ms_c", C.c_double), ("ms_e", C.c_double), ("ms_pack", C.c_double), ("ms_refine", C.c_double),
                 ("ms_total", C.c_double), ("objective_passes", C.c_longlong), ("joint_taken", C.c_int),
-                ("e_joint", C.c_double), ("ms_joint", C.c_double)]
+                ("e_before_joint", C.c_double), ("e_joint", C.c_double), ("ms_joint", C.c_double)]
 
 
 # nntc_b200_set_option's options (include/nntc_b200.h, enum nntc_b200_option)
 OPT_REFERENCE_SHAPED_ASSEMBLY = 0
 OPT_MIXED_PRECISION_GRAM = 1
 OPT_ADJOINT_CG = 2
+OPT_MIXED_OBJECTIVE = 3
 
 
 def feature_count(c0: int, c1: int) -> int:

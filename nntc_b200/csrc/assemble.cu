@@ -538,6 +538,48 @@ __global__ void __launch_bounds__(GATHER_THREADS, 7) k_gather_level1(Planes P, c
 }
 
 // Launch both passes for every plane: the per-site terms, then the per-(texel, slot) gather.
+// The fractional sites' float targets at K in d->site_tgt ([fractional site][nout], planes in order), formed when the
+// device does not hold them for this K yet: read by the assembly's site pass and the mixed-precision objective.
+int ensure_site_targets(nntc_b200_device* d, int k, int level0)
+{
+    if (d->site_tgt_kc == k || k == 0)
+        return NNTC_B200_OK;
+    TargetOffsets O{};
+    long long ft = 0;
+    for (int i = 0; i < (int)d->planes.size(); i++)
+    {
+        O.site0[i] = ft;
+        ft += (long long)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0 * k;
+    }
+    O.site0[d->planes.size()] = ft;
+    Planes T = planes_for(d, level0, [&](int i) {
+        const DevPlane& p = d->planes[(size_t)i];
+        return (size_t)p.w0 * p.h0 * (size_t)k;
+    });
+    T.kc = k;
+    const int tblocks = (int)(T.start[T.n] / SITE_THREADS);
+#define NB_TARGETS(NO)                                                                                                \
+    case NO:                                                                                                          \
+        k_site_targets<NO><<<tblocks, SITE_THREADS, 0, d->stream>>>(T, d->site_tgt, O);                               \
+        break;
+    switch (d->nout)
+    {
+        NB_TARGETS(3)
+        NB_TARGETS(6)
+        NB_TARGETS(9)
+        NB_TARGETS(12)
+        NB_TARGETS(15)
+        NB_TARGETS(18)
+    default:
+        set_error(NNTC_B200_ERR_STATE, "a material holds 1..6 RGB textures");
+        return NNTC_B200_ERR_STATE;
+    }
+#undef NB_TARGETS
+    NB_LAUNCHED();
+    d->site_tgt_kc = k;
+    return NNTC_B200_OK;
+}
+
 int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono,
                    int slots)
 {
@@ -604,43 +646,15 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     // the fractional sites' targets, formed on the first assembly at this K
     A.tgt = d->site_tgt;
     {
-        TargetOffsets O{};
         long long ft = 0;
         for (int i = 0; i < S.n; i++)
         {
-            O.site0[i] = A.tsite0[i] = ft;
+            A.tsite0[i] = ft;
             ft += (long long)d->planes[(size_t)i].w0 * d->planes[(size_t)i].h0 * k;
         }
-        O.site0[S.n] = A.tsite0[S.n] = ft;
-        if (d->site_tgt_kc != k && k > 0)
-        {
-            Planes T = planes_for(d, level0, [&](int i) {
-                const DevPlane& p = d->planes[(size_t)i];
-                return (size_t)p.w0 * p.h0 * (size_t)k;
-            });
-            T.kc = k;
-            const int tblocks = (int)(T.start[T.n] / SITE_THREADS);
-#define NB_TARGETS(NO)                                                                                                \
-    case NO:                                                                                                          \
-        k_site_targets<NO><<<tblocks, SITE_THREADS, 0, d->stream>>>(T, d->site_tgt, O);                               \
-        break;
-            switch (d->nout)
-            {
-                NB_TARGETS(3)
-                NB_TARGETS(6)
-                NB_TARGETS(9)
-                NB_TARGETS(12)
-                NB_TARGETS(15)
-                NB_TARGETS(18)
-            default:
-                set_error(NNTC_B200_ERR_STATE, "a material holds 1..6 RGB textures");
-                return NNTC_B200_ERR_STATE;
-            }
-#undef NB_TARGETS
-            NB_LAUNCHED();
-        }
-        d->site_tgt_kc = k;
+        A.tsite0[S.n] = ft;
     }
+    NB_TRY(ensure_site_targets(d, k, level0));
     const int sblocks = (int)(S.start[S.n] / SITE_THREADS);
     SiteDecoder W{};
     const int nin = d->nin, c0 = d->c0, c1 = d->c1;

@@ -136,6 +136,7 @@ struct nntc_b200_device
     int reference_shaped_assembly = 0;   // 1: the per-texel gather of the reference's shape (same bits, slower)
     int mixed_gram = 0;                  // 1: block (a)'s sums on the tensor cores, BF16 hi + lo (gram_tc.cu)
     int adjoint_cg = 0;                  // 1: blocks (b) and (c')'s conjugate gradients matrix-free (adjoint_cg.cu)
+    int mixed_objective = 0;             // 1: the objective's decode in FP32, its squares summed in FP64
     double* cov = nullptr;               // the init's moment partials, [entry][COV_GRID]
     void* basis = nullptr;               // the init's principal directions, peaks and divisor (1 KB)
     unsigned long long* hist = nullptr;  // the percentile histogram (init0, palette mode)

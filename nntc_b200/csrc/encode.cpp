@@ -73,6 +73,7 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
     NB_CUDA(cudaEventCreate(&j0));
     NB_CUDA(cudaEventCreate(&j1));
     NB_CUDA(cudaEventRecord(j0, d->stream));
+    r->e_before_joint = e_ship;
     NB_TRY(snapshot(d, true));
     const nntc_b200_model keep_m = *m;
     auto restore = [&]() -> int {
@@ -182,17 +183,19 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     struct FormScope
     {
         nntc_b200_device* d;
-        int gram, cg;
+        int gram, cg, obj;
         ~FormScope()
         {
             d->mixed_gram = gram;
             d->adjoint_cg = cg;
+            d->mixed_objective = obj;
         }
-    } form_scope{ d, d->mixed_gram, d->adjoint_cg };
+    } form_scope{ d, d->mixed_gram, d->adjoint_cg, d->mixed_objective };
     if (a->form == 1)
     {
         d->mixed_gram = 1;
         d->adjoint_cg = 1;
+        d->mixed_objective = 1;
     }
     else if (a->form != 0)
     {
@@ -204,6 +207,10 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     NB_CUDA(cudaEventCreate(&t1));
     NB_CUDA(cudaEventRecord(t0, d->stream));
     const long long passes0 = nntc_b200_objective_passes();
+    // The fractional sites' targets (a pure function of the source chain and K) are formed inside every encode, so an
+    // encode's time does not depend on what an earlier encode on the same device model left behind.
+    d->site_tgt_kc = -1;
+    d->obj_tgt_kc = -1;
 
     // The start state (src/main.cpp:1838-1915): no decoder (the device's is zero), level 0's grid [-1, 1] under bc8,
     // no level-1 grid yet.

@@ -355,6 +355,103 @@ __global__ void __launch_bounds__(OBJ_P_THREADS, 5)
     }
 }
 
+// The mixed-precision objective (the adjoint form): the sites' samples with the float tap rule of the assembly
+// (tap_at, blend), every output row's dot product in FP32 fused multiply-adds with the decoder as a launch parameter,
+// the fractional sites' float targets of the assembly (d->site_tgt), and each residual squared and summed in FP64. E
+// agrees with the FP64 objective to about 1e-7 relative; what decides on E (the stops, the acceptance of a repack pass)
+// sees the same E within tolerances four orders coarser.
+struct ObjDecoderF
+{
+    float w[MAX_NOUT * 24];
+    float b[MAX_NOUT];
+    float cw[MAX_NOUT];
+};
+
+struct ObjTargetsF
+{
+    const float* t;                    // [fractional site][NOUT]
+    long long site0[MAX_PLANES + 1];
+};
+
+template <int NOUT>
+__global__ void __launch_bounds__(OBJ_P_THREADS, 6)
+    k_objective_f32(Planes P, ObjDecoderF W, double* partial, const __grid_constant__ ObjTargetsF T)
+{
+    __shared__ double red[32];
+    const int c0 = P.c0, c1 = P.c1, kc = P.kc;
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long local = base - P.start[pl] + threadIdx.x;
+    double weighted = 0.0, centre = 0.0, fractional = 0.0;
+    if (local < (long long)V.w0 * V.h0)
+    {
+        const int px = (int)(local % V.w0), py = (int)(local / V.w0);
+        for (int j = 0; j <= kc; j++)
+        {
+            float dx, dy;
+            site_offset(kc, j, px, py, dx, dy);
+            float s[MAX_CH] = { 0.0f, 0.0f, 0.0f, 0.0f }, c[MAX_CH] = { 0.0f, 0.0f, 0.0f, 0.0f };
+            blend_u<MAX_CH>(V.v1, V.w1, c1, tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1), c);
+            if (j == 0)
+            {
+#pragma unroll
+                for (int i = 0; i < MAX_CH; i++)
+                    if (i < c0)
+                        s[i] = __ldg(V.v0 + local * c0 + i);
+            }
+            else
+                blend_u<MAX_CH>(V.v0, V.w0, c0, tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0), s);
+            float acc[NOUT];
+#pragma unroll
+            for (int r = 0; r < NOUT; r++)
+                acc[r] = W.b[r];
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+#pragma unroll
+                for (int r = 0; r < NOUT; r++)
+                    acc[r] = __fmaf_rn(W.w[r * 24 + h], c[h], acc[r]);
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+#pragma unroll
+                for (int r = 0; r < NOUT; r++)
+                    acc[r] = __fmaf_rn(W.w[r * 24 + 4 + h], s[h], acc[r]);
+#pragma unroll
+            for (int h = 0; h < 16; h++)
+            {
+                const float sc = s[h / 4] * c[h % 4];
+#pragma unroll
+                for (int r = 0; r < NOUT; r++)
+                    acc[r] = __fmaf_rn(W.w[r * 24 + 8 + h], sc, acc[r]);
+            }
+            const float* tg = j == 0 ? V.src + (size_t)local * NOUT
+                                     : T.t + (size_t)(T.site0[pl] + local * kc + (j - 1)) * NOUT;
+#pragma unroll
+            for (int r = 0; r < NOUT; r++)
+            {
+                const double e = (double)(acc[r] - __ldg(tg + r));
+                weighted = fma((double)W.cw[r] * e, e, weighted);
+                if (j == 0)
+                    centre = fma(e, e, centre);
+                else
+                    fractional = fma(e, e, fractional);
+            }
+        }
+    }
+    const double a = block_sum(weighted, red);
+    const double b = block_sum(centre, red);
+    const double c = block_sum(fractional, red);
+    if (threadIdx.x == 0)
+    {
+        const size_t nb = gridDim.x;
+        partial[blockIdx.x] = a;
+        partial[nb + blockIdx.x] = b;
+        partial[2 * nb + blockIdx.x] = c;
+    }
+}
+
+int ensure_site_targets(nntc_b200_device* d, int k, int level0);
+
 // One block per plane: the plane's block partials added in a fixed order (a strided pass, then a fixed tree).
 __global__ void k_objective_reduce(Planes P, const double* partial, int nblocks, double* out, int bthreads)
 {
@@ -520,7 +617,7 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
         }
         T.site0[P.n] = ft;
     }
-    if (d->obj_tgt_kc != k && k > 0 && bthreads == OBJ_P_THREADS)
+    if (d->obj_tgt_kc != k && k > 0 && bthreads == OBJ_P_THREADS && !d->mixed_objective)
     {
         Planes F = planes_for(d, 0, [&](int i) {
             const DevPlane& p = d->planes[(size_t)i];
@@ -539,6 +636,39 @@ int objective_sums(nntc_b200_device* d, int k, std::vector<double>& acc, double*
         }
         NB_LAUNCHED();
         d->obj_tgt_kc = k;
+    }
+    if (d->mixed_objective && bthreads == OBJ_P_THREADS)
+    {
+        NB_TRY(ensure_site_targets(d, k, 0));
+        ObjDecoderF F{};
+        for (int i = 0; i < nout * 24; i++)
+            F.w[i] = (float)W.w[i];
+        for (int r = 0; r < nout; r++)
+        {
+            F.b[r] = d->host_bias[r];
+            F.cw[r] = d->m.cw[r];
+        }
+        ObjTargetsF TF{};
+        TF.t = d->site_tgt;
+        for (int i = 0; i <= P.n; i++)
+            TF.site0[i] = T.site0[i];
+        NB_TRY(ktimer_begin(d, NNTC_B200_K_OBJECTIVE));
+        switch (nout)
+        {
+        case 3: k_objective_f32<3><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, F, d->obj_partial, TF); break;
+        case 6: k_objective_f32<6><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, F, d->obj_partial, TF); break;
+        case 9: k_objective_f32<9><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, F, d->obj_partial, TF); break;
+        case 12: k_objective_f32<12><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, F, d->obj_partial, TF); break;
+        case 15: k_objective_f32<15><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, F, d->obj_partial, TF); break;
+        default: k_objective_f32<18><<<nblocks, OBJ_P_THREADS, 0, d->stream>>>(P, F, d->obj_partial, TF); break;
+        }
+        NB_TRY(ktimer_end(d));
+        NB_LAUNCHED();
+        k_objective_reduce<<<P.n, 256, 0, d->stream>>>(P, d->obj_partial, nblocks, sums, bthreads);
+        NB_LAUNCHED();
+        NB_TRY(block_end(d, ms));
+        acc.assign((size_t)3 * P.n, 0.0);
+        return download(d, acc.data(), sums, acc.size() * sizeof(double));
     }
     NB_TRY(ktimer_begin(d, NNTC_B200_K_OBJECTIVE));
     switch (nout)

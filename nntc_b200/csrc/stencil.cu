@@ -1253,6 +1253,11 @@ int nntc_b200_set_option(nntc_b200_device* d, int option, int value)
         d->adjoint_cg = value != 0;
         return NNTC_B200_OK;
     }
+    if (option == NNTC_B200_OPT_MIXED_OBJECTIVE)
+    {
+        d->mixed_objective = value != 0;
+        return NNTC_B200_OK;
+    }
     set_error(NNTC_B200_ERR_ARG, "no such option");
     return NNTC_B200_ERR_ARG;
 }

@@ -249,7 +249,7 @@ def small(seed: int, width: int, height: int, textures: int = 1, c0: int = 2, c1
     return Material(f"{textures}x{width}x{height}", tex, c0, c1, k, mip_min).build()
 
 
-def write_png(path: str, rgb8) -> None:
+def write_png(path: str, rgb8, level: int = 6) -> None:
     """An 8-bit RGB PNG (zlib-compressed, filter 0 rows): what the reference's encoder reads as its input."""
     import struct
     import zlib
@@ -264,18 +264,18 @@ def write_png(path: str, rgb8) -> None:
     with open(path, "wb") as f:
         f.write(b"\x89PNG\r\n\x1a\n")
         f.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)))
-        f.write(chunk(b"IDAT", zlib.compress(raw, 6)))
+        f.write(chunk(b"IDAT", zlib.compress(raw, level)))
         f.write(chunk(b"IEND", b""))
 
 
-def save_material(material, directory: str):
-    """The material's textures as PNGs, in order; returns the paths."""
+def save_material(material, directory: str, level: int = 6):
+    """The material's textures as PNGs (zlib level `level`), in order; returns the paths."""
     import os
 
     os.makedirs(directory, exist_ok=True)
     paths = []
     for i, t in enumerate(material.textures):
         p = os.path.join(directory, f"tex{i}.png")
-        write_png(p, t)
+        write_png(p, t, level)
         paths.append(p)
     return paths
