@@ -229,8 +229,9 @@ int nntc_b200_objective_check_host(nntc_b200_device* d, const nntc_b200_model* m
  * them (e_plane = sums[0] / (sum cw (1 + k) w0 h0)). Both kernels are queued on `stream` (a cudaStream_t; 0 is the
  * legacy default stream) and the call returns without waiting. The only scratch is a fixed static device array of
  * 1.5 MiB, hence the limit of NNTC_B200_NOALLOC_MAX_PIXELS pixels per call; a larger plane is rejected with
- * NNTC_B200_ERR_ARG and a message naming the limit. The first call on a device does its setup (it looks up the
- * scratch's address, which loads the library's device code on that device) and should come before any stream capture.
+ * NNTC_B200_ERR_ARG and a message naming the limit. Every call looks up the scratch's address on the current device
+ * (cudaGetSymbolAddress, which allocates nothing); the first call on a device also loads the library's device code
+ * there, so it should come before any stream capture.
  * Calls in flight at the same time on one device (different streams, or host threads without ordering) share that
  * scratch and race: order them, e.g. on one stream. */
 #define NNTC_B200_NOALLOC_MAX_PIXELS (4096LL * 4096LL)

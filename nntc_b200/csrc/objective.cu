@@ -822,34 +822,19 @@ namespace nb
 {
 
 constexpr long long NOALLOC_MAX_BLOCKS = NNTC_B200_NOALLOC_MAX_PIXELS / OBJ_THREADS;
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
 // Every word a call reads is written earlier in the same call (k_objective writes each block's three partials,
 // k_objective_reduce reads only those), so nothing here needs to start at zero.
 static __device__ __align__(256) double g_noalloc_partial[3 * NOALLOC_MAX_BLOCKS];
 
-static std::mutex g_noalloc_mutex;
-static double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
-
-// The scratch's device address on the current device, looked up once per device with that device current.
+// The scratch's device address on the current device, looked up on every call with that device current: a stored
+// address could outlive the context it belongs to (a device reset, another context on the same ordinal), and the
+// lookup allocates nothing.
 static int noalloc_scratch(double** out)
 {
-    int dev = -1;
-    NB_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-    {
-        set_error(NNTC_B200_ERR_ARG, "objective_plane_noalloc: device ordinal " + std::to_string(dev) +
-                                         " is beyond the " + std::to_string(NOALLOC_MAX_DEVICES) + " it keeps");
-        return NNTC_B200_ERR_ARG;
-    }
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev])
-    {
-        void* p = nullptr;
-        NB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partial));
-        g_noalloc_addr[dev] = (double*)p;
-    }
-    *out = g_noalloc_addr[dev];
+    void* p = nullptr;
+    NB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partial));
+    *out = (double*)p;
     return NNTC_B200_OK;
 }
 

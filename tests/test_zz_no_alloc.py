@@ -29,7 +29,8 @@ def close(a, b):
     return abs(a - b) <= TOL * max(abs(a), abs(b))
 
 
-@pytest.mark.parametrize("textures,c0,c1,w,h,k", [(2, 4, 4, 72, 40, 4), (1, 2, 4, 61, 37, 4), (6, 4, 4, 48, 44, 1)])
+@pytest.mark.parametrize("textures,c0,c1,w,h,k", [(2, 4, 4, 72, 40, 4), (1, 2, 4, 61, 37, 4), (6, 4, 4, 48, 44, 1),
+                                                  (3, 3, 2, 50, 34, 2), (2, 1, 3, 40, 28, 0)])
 def test_noalloc_matches_objective_eval(textures, c0, c1, w, h, k):
     import torch
 
@@ -67,8 +68,10 @@ def test_noalloc_matches_objective_eval(textures, c0, c1, w, h, k):
                 out = sums.cpu().numpy()
                 assert close(out[0] / (sum_cw * (pixels * (1 + k))), ref.e_plane[i]), (i, rep)
                 assert close(out[1] / (pixels * nout), ref.centre_plane[i]), (i, rep)
-                if i == 0:
+                if i == 0 and k > 0:
                     assert close(out[2] / (pixels * nout * k), ref.sampled_mse), rep
+                elif k == 0:
+                    assert out[2] == 0.0, rep   # no fractional sites: their sum is an exact zero
 
 
 def test_noalloc_rejects_a_plane_above_its_limit():
