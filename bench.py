@@ -346,8 +346,28 @@ def main():
 
     if rank == 0:
         hbm, tf, src = peaks()
+        fp64 = C.c_double()
+        fp32 = C.c_double()
+        check(L.nntc_b200_measure_fma_peaks(C.byref(fp64), C.byref(fp32)), "measure_fma_peaks")
+        pipes = {"fp64_tflops": round(fp64.value, 2), "fp32_tflops": round(fp32.value, 2),
+                 "how": "nntc_b200_measure_fma_peaks: 8 independent FMA chains per thread, 4 blocks per SM, CUDA events"}
         dom = max(stats, key=lambda k: stats[k][1])
         roof = roofline(dom, stats[dom], mat, hbm, tf, src)
+        fractions = {}
+        for name, st in stats.items():
+            if st[0] == 0:
+                continue
+            per_launch_s = st[1] / st[0] / 1000.0
+            entry = {"ms_per_launch": round(st[1] / st[0], 4),
+                     "hbm_frac": round(algorithmic_bytes(name, mat) / per_launch_s / 1e9 / hbm, 4),
+                     "binding": BINDING.get(name)}
+            fl = algorithmic_flops(name, mat)
+            if fl:
+                pipe = "fp32" if headline == "adjoint" else "fp64"
+                peak = fp32.value if pipe == "fp32" else fp64.value
+                entry["compute"] = {"pipe": pipe, "achieved_tflops": round(fl / per_launch_s / 1e12, 3),
+                                    "peak_tflops": round(peak, 2), "frac": round(fl / per_launch_s / 1e12 / peak, 4)}
+            fractions[name] = entry
         nt = len(mat.textures)
         psnr_h = [round(x, 3) for x in results[-1].psnr[:nt]]
         psnr_o = [round(x, 3) for x in other_results[-1].psnr[:nt]]
@@ -386,6 +406,8 @@ def main():
                             "state, asset (.dds + JSON) written to disk"},
             "gpu_launches": launches,
             "roofline": roof,
+            "kernel_fractions": fractions,
+            "pipe_peaks": pipes,
             "clocks": clocks.summary(),
         }
         if world == 1 and not args.no_reference_cuda:
@@ -470,6 +492,18 @@ def roofline(name, stat, mat, hbm, tf, src):
             else "no ncu DRAM figure recorded for this group's current kernels",
             "binding": BINDING.get(name), "bytes_per_launch": per, "launches": launches,
             "ms_per_launch": round(ms / launches, 4)}
+
+
+def algorithmic_flops(name, mat):
+    """Floating-point operations a launch of a pipe-bound group does (every plane of the chain), where they are the
+    work that matters: the objective's per-site sampling, decode and squared residuals."""
+    c0, c1, nout, k = mat.c0, mat.c1, 3 * len(mat.textures), mat.k
+    nin = c1 + c0 + c0 * c1
+    t0 = sum(p[0] * p[1] for p in mat.planes)
+    if name == "objective":
+        per_site = 2 * nout * nin + c0 * c1 + 5 * nout
+        return t0 * ((1 + k) * per_site + 8 * c1 * (1 + k) + 8 * c0 * k)
+    return 0
 
 
 def algorithmic_bytes(name, mat):

@@ -353,6 +353,10 @@ enum nntc_b200_kernel
     NNTC_B200_K_MATVEC0,         /* one conjugate-gradient product over every plane, block (c') (level 0) */
     NNTC_B200_K_COUNT
 };
+/* The measured fused-multiply-add peaks of the current device's FP64 and FP32 vector pipes, in TFLOP/s (2 flops per
+ * FMA): eight independent chains per thread, four blocks per SM, timed with CUDA events. No counterpart in the
+ * reference; the denominators of the compute fractions the benchmark reports for pipe-bound kernels. */
+int nntc_b200_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 /* on != 0 brackets every launch of the kernels above with a pair of CUDA events; stats accumulate until reset. */
 int nntc_b200_kernel_timing(nntc_b200_device* d, int on);
 /* The launches of `kernel` since the last reset and their summed event time; reset != 0 clears every kernel's. */
