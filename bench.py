@@ -273,11 +273,13 @@ def main():
 
     headline, other = args.form, ("plain" if args.form == "adjoint" else "adjoint")
     ea = encode_args(L, headline)
-    # the other form first, a few encodes, for the form ratio and the PSNR delta
+    # the other form first, a few encodes, for the form ratio and the PSNR delta (none with --compare-steps 0)
     ea_other = encode_args(L, other)
-    encode_resident(ea_other)
-    other_results = [encode_resident(ea_other) for _ in range(args.compare_steps)]
-    other_ms = statistics.median(r.ms_total for r in other_results)
+    other_results = []
+    if args.compare_steps > 0:
+        encode_resident(ea_other)
+        other_results = [encode_resident(ea_other) for _ in range(args.compare_steps)]
+    other_ms = statistics.median(r.ms_total for r in other_results) if other_results else None
 
     for _ in range(args.warmup):
         encode_resident(ea)
@@ -370,19 +372,20 @@ def main():
             fractions[name] = entry
         nt = len(mat.textures)
         psnr_h = [round(x, 3) for x in results[-1].psnr[:nt]]
-        psnr_o = [round(x, 3) for x in other_results[-1].psnr[:nt]]
         head_ms = device_ms / args.steps
         forms = {headline: {"ms_per_encode": round(head_ms, 2), "mpix_s": round(mpix / (head_ms / 1000), 6),
-                            "psnr": psnr_h, "e_ship": results[-1].e_ship},
-                 other: {"ms_per_encode": round(other_ms, 2), "mpix_s": round(mpix / (other_ms / 1000), 6),
-                         "psnr": psnr_o, "e_ship": other_results[-1].e_ship, "steps": args.compare_steps}}
-        adj = forms["adjoint"]
-        pln = forms["plain"]
-        forms["adjoint_over_plain"] = round(pln["ms_per_encode"] / adj["ms_per_encode"], 4)
-        forms["psnr_delta_db"] = [round(a - b, 3) for a, b in zip(adj["psnr"], pln["psnr"])]
-        adj_res = results[-1] if headline == "adjoint" else other_results[-1]
-        forms["joint_pass"] = {"taken": adj_res.joint_taken, "e_reached": adj_res.e_joint,
-                               "ms": round(adj_res.ms_joint, 2)}
+                            "psnr": psnr_h, "e_ship": results[-1].e_ship}}
+        if other_results:
+            psnr_o = [round(x, 3) for x in other_results[-1].psnr[:nt]]
+            forms[other] = {"ms_per_encode": round(other_ms, 2), "mpix_s": round(mpix / (other_ms / 1000), 6),
+                            "psnr": psnr_o, "e_ship": other_results[-1].e_ship, "steps": args.compare_steps}
+            adj, pln = forms["adjoint"], forms["plain"]
+            forms["adjoint_over_plain"] = round(pln["ms_per_encode"] / adj["ms_per_encode"], 4)
+            forms["psnr_delta_db"] = [round(a - b, 3) for a, b in zip(adj["psnr"], pln["psnr"])]
+        adj_res = results[-1] if headline == "adjoint" else (other_results[-1] if other_results else None)
+        if adj_res is not None:
+            forms["joint_pass"] = {"taken": adj_res.joint_taken, "e_before": adj_res.e_before_joint,
+                                   "e_reached": adj_res.e_joint, "ms": round(adj_res.ms_joint, 2)}
         line = {
             "metric": "encode Mpix/s", "value": round(value, 6), "unit": "Mpix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(head_ms, 3),
