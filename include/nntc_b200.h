@@ -274,7 +274,8 @@ typedef struct nntc_b200_encode_args
     float luma[3];         /* 0.299, 0.587, 0.114 */
     /* 0: the plain form, the reference's arithmetic (FP64 stencils and sums). 1: the adjoint + mixed-precision form:
      * block (a)'s sums on the tensor cores (NNTC_B200_OPT_MIXED_PRECISION_GRAM), the conjugate gradients matrix-free
-     * in FP32 (NNTC_B200_OPT_ADJOINT_CG), the objective's decode in FP32 (NNTC_B200_OPT_MIXED_OBJECTIVE), and after
+     * in FP32 (NNTC_B200_OPT_ADJOINT_CG), the objective's decode in FP32 (NNTC_B200_OPT_MIXED_OBJECTIVE), the
+     * stencils of the quantised sweeps in FP32 (NNTC_B200_OPT_FP32_STENCIL), and after
      * the repack passes one joint latent / decoder pass (bc8): a step
      * of both latents along their preconditioned objective gradient with the decoder re-solved, the best of three
      * step lengths, re-packed and refined, kept only when the shipped E falls. Has no counterpart in the reference. */
@@ -333,7 +334,11 @@ enum nntc_b200_option
     /* 1: the objective's per-site decode in FP32 (the assembly's float tap rule and float targets) with every
      * residual's square summed in FP64 (the adjoint form; E to about 1e-7 relative). 0 (default): the decode in FP64 on
      * the double u-space sampling rule (src/objective.cu:97-211). */
-    NNTC_B200_OPT_MIXED_OBJECTIVE = 3
+    NNTC_B200_OPT_MIXED_OBJECTIVE = 3,
+    /* 1: blocks (b) and (c') assemble their stencils in FP32 (the gathers' sums and the stored blocks), which the
+     * quantised sweeps then read at half the bytes; the BC refinement's assembly stays FP64 (the adjoint form). 0
+     * (default): FP64, the reference's bits (src/solve_level1.cu:259-581). */
+    NNTC_B200_OPT_FP32_STENCIL = 4
 };
 int nntc_b200_set_option(nntc_b200_device* d, int option, int value);
 

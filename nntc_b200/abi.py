@@ -91,6 +91,7 @@ OPT_REFERENCE_SHAPED_ASSEMBLY = 0
 OPT_MIXED_PRECISION_GRAM = 1
 OPT_ADJOINT_CG = 2
 OPT_MIXED_OBJECTIVE = 3
+OPT_FP32_STENCIL = 4
 
 
 def feature_count(c0: int, c1: int) -> int:

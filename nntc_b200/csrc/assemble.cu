@@ -292,6 +292,7 @@ struct GatherArgs
     // the monomial matrices (c x c, row-major) at their monomial's slot of the fixed layout, unused slots left out:
     // with the expansion unrolled every entry is a constant-bank operand, no loads
     double mono[MAX_MONO][MAX_CH * MAX_CH];
+    float monof[MAX_MONO][MAX_CH * MAX_CH];   // the same in FP32, for the FP32 stencil of the adjoint form
     const int4* tab;      // the visit tables of this level and K
     GatherTable gt;
     unsigned tabled;      // bit i: plane i's interior texels may use the tables
@@ -333,7 +334,22 @@ __device__ __forceinline__ void stencil_texel(long long pos, int w, int h, int& 
 // neighbour, in site order, expanded into the slot's block; the self-slot thread also gathers the gradient. Threads
 // take the texels in the stencil's colour-major order, so a warp's texels share a parity class (one visit table) and
 // its stores are contiguous.
-template <bool LEVEL0>
+template <typename TS>
+__device__ __forceinline__ TS mono_entry(const GatherArgs& A, int L, int e);
+template <>
+__device__ __forceinline__ double mono_entry<double>(const GatherArgs& A, int L, int e)
+{
+    return A.mono[L][e];
+}
+template <>
+__device__ __forceinline__ float mono_entry<float>(const GatherArgs& A, int L, int e)
+{
+    return A.monof[L][e];
+}
+
+// TS: the stencil's stored type and the sums' type - double for the plain form (the reference's bits), float for the
+// adjoint form (the sweeps then read half the bytes; the gradient stays in double either way).
+template <bool LEVEL0, typename TS>
 __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A)
 {
     // Block order: (region, colour, slot) with the slot fastest. The five slots of one run of texels, and the four
@@ -371,14 +387,14 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
     {
         // no neighbour in this direction: the reference's block is zero (no site touches both)
         for (int e = 0; e < cc; e++)
-            V.stencil[(size_t)(slot * cc + e) * T + sp] = 0.0;
+            reinterpret_cast<TS*>(V.stencil)[(size_t)(slot * cc + e) * T + sp] = (TS)0;
         return;
     }
 
-    double sums[MAX_MONO];
+    TS sums[MAX_MONO];
 #pragma unroll
     for (int i = 0; i < MAX_MONO; i++)
-        sums[i] = 0.0;
+        sums[i] = (TS)0;
     double g[MAX_CH];
 #pragma unroll
     for (int a = 0; a < MAX_CH; a++)
@@ -401,18 +417,18 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
                 if (a < c)
                     g[a] += (double)w_self * ts[a];
         }
-        const double scale = (double)w_self * (double)w_other;
-        sums[0] += scale * 1.0;
+        const TS scale = (TS)w_self * (TS)w_other;
+        sums[0] += scale * (TS)1;
 #pragma unroll
         for (int i = 0; i < MAX_CH; i++)
             if (i < ny_)
-                sums[1 + i] += scale * (double)y[i];
+                sums[1 + i] += scale * (TS)y[i];
 #pragma unroll
         for (int p = 0; p < 10; p++)
         {
             const int i = pair_i(p), k2 = pair_k(p);
             if (k2 < ny_)
-                sums[5 + p] += scale * ((double)y[i] * (double)y[k2]);
+                sums[5 + p] += scale * ((TS)y[i] * (TS)y[k2]);
         }
     };
     auto visit = [&](int px, int py, int j, float w_self, float w_other) {
@@ -499,27 +515,27 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
 #pragma unroll
     for (int part = 0; part < MAX_CH * MAX_CH / PART; part++)
     {
-        double blk[PART];
+        TS blk[PART];
 #pragma unroll
         for (int e = 0; e < PART; e++)
-            blk[e] = 0.0;
+            blk[e] = (TS)0;
 #pragma unroll
         for (int L = 0; L < MAX_MONO; L++)
         {
             if (!mono_used(L, ny_))
                 continue;
-            const double s = sums[L];
-            if (s == 0.0)
+            const TS s = sums[L];
+            if (s == (TS)0)
                 continue;
 #pragma unroll
             for (int e = 0; e < PART; e++)
                 if (part * PART + e < cc)
-                    blk[e] += s * A.mono[L][part * PART + e];
+                    blk[e] += s * mono_entry<TS>(A, L, part * PART + e);
         }
 #pragma unroll
         for (int e = 0; e < PART; e++)
             if (part * PART + e < cc)
-                V.stencil[(size_t)(slot * cc + part * PART + e) * T + sp] = blk[e];
+                reinterpret_cast<TS*>(V.stencil)[(size_t)(slot * cc + part * PART + e) * T + sp] = blk[e];
     }
     if (LEVEL0)
         store_grad();
@@ -527,14 +543,16 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
 
 // The two levels' kernels: level 1 capped at seven blocks per SM (its expansion is split for that), level 0 left at
 // the register count it takes unconstrained (a cap made it spill and run slower).
+template <typename TS>
 __global__ void __launch_bounds__(GATHER_THREADS) k_gather_level0(Planes P, const __grid_constant__ GatherArgs A)
 {
-    gather_body<true>(P, A);
+    gather_body<true, TS>(P, A);
 }
 
+template <typename TS>
 __global__ void __launch_bounds__(GATHER_THREADS, 7) k_gather_level1(Planes P, const __grid_constant__ GatherArgs A)
 {
-    gather_body<false>(P, A);
+    gather_body<false, TS>(P, A);
 }
 
 // Launch both passes for every plane: the per-site terms, then the per-(texel, slot) gather.
@@ -581,7 +599,7 @@ int ensure_site_targets(nntc_b200_device* d, int k, int level0)
 }
 
 int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono,
-                   int slots)
+                   int slots, bool f32)
 {
     Planes S = planes_for(d, level0, [&](int i) {
         const DevPlane& p = d->planes[(size_t)i];
@@ -600,6 +618,8 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
             if (mono_used(L, ny))
             {
                 std::memcpy(G.mono[L], mono + (size_t)q * c * c, (size_t)c * c * sizeof(double));
+                for (int e = 0; e < c * c; e++)
+                    G.monof[L][e] = (float)G.mono[L][e];
                 q++;
             }
         if (q != nmono)
@@ -701,10 +721,14 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
     }
     G.bstart[P_texels.n] = blocks;
     const unsigned grid = (unsigned)blocks;
-    if (level0)
-        k_gather_level0<<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+    if (level0 && f32)
+        k_gather_level0<float><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+    else if (level0)
+        k_gather_level0<double><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+    else if (f32)
+        k_gather_level1<float><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
     else
-        k_gather_level1<<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
+        k_gather_level1<double><<<grid, GATHER_THREADS, 0, d->stream>>>(P_texels, G);
     NB_LAUNCHED();
     return NNTC_B200_OK;
 }

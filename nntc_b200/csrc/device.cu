@@ -888,7 +888,16 @@ int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double
     if (stencil)
     {
         std::vector<double> soa(t * per);
-        NB_TRY(download(d, soa.data(), w.stencil, soa.size() * sizeof(double)));
+        if (d->sten_f32[level0 ? 1 : 0])
+        {
+            // an FP32 stencil (the adjoint form's), widened
+            std::vector<float> f(t * per);
+            NB_TRY(download(d, f.data(), w.stencil, f.size() * sizeof(float)));
+            for (size_t q = 0; q < f.size(); q++)
+                soa[q] = (double)f[q];
+        }
+        else
+            NB_TRY(download(d, soa.data(), w.stencil, soa.size() * sizeof(double)));
         // back from the colour-major SoA order to the reference's [texel][slot][i][j]
         for (size_t i = 0; i < t; i++)
         {

@@ -137,6 +137,8 @@ struct nntc_b200_device
     int mixed_gram = 0;                  // 1: block (a)'s sums on the tensor cores, BF16 hi + lo (gram_tc.cu)
     int adjoint_cg = 0;                  // 1: blocks (b) and (c')'s conjugate gradients matrix-free (adjoint_cg.cu)
     int mixed_objective = 0;             // 1: the objective's decode in FP32, its squares summed in FP64
+    int mixed_stencil = 0;               // 1: blocks (b) and (c') assemble an FP32 stencil (gathers in FP32)
+    bool sten_f32[2] = { false, false }; // what the last assembly of level 1 / level 0 stored: FP32 or FP64
     double* cov = nullptr;               // the init's moment partials, [entry][COV_GRID]
     void* basis = nullptr;               // the init's principal directions, peaks and divisor (1 KB)
     unsigned long long* hist = nullptr;  // the percentile histogram (init0, palette mode)

@@ -183,19 +183,21 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     struct FormScope
     {
         nntc_b200_device* d;
-        int gram, cg, obj;
+        int gram, cg, obj, sten;
         ~FormScope()
         {
             d->mixed_gram = gram;
             d->adjoint_cg = cg;
             d->mixed_objective = obj;
+            d->mixed_stencil = sten;
         }
-    } form_scope{ d, d->mixed_gram, d->adjoint_cg, d->mixed_objective };
+    } form_scope{ d, d->mixed_gram, d->adjoint_cg, d->mixed_objective, d->mixed_stencil };
     if (a->form == 1)
     {
         d->mixed_gram = 1;
         d->adjoint_cg = 1;
         d->mixed_objective = 1;
+        d->mixed_stencil = 1;
     }
     else if (a->form != 0)
     {

@@ -359,8 +359,18 @@ struct Red
     double* scalars;      // [plane][S_COUNT]
 };
 
+// One coefficient of the stencil as stored: FP64 (the plain form) or FP32 (the adjoint form's quantised sweeps read a
+// single-precision stencil, half the bytes), widened to double for the sums that read it.
+template <typename TS>
+__device__ __forceinline__ double sten(const PlaneView& V, size_t idx)
+{
+    return (double)reinterpret_cast<const TS*>(V.stencil)[idx];
+}
+
+
 // ---- ridge, preconditioner ----------------------------------------------------------------------------------------
 
+template <typename TS>
 __global__ void __launch_bounds__(THREADS) k_diag(Planes P, Red R)
 {
     __shared__ double sh[3 * 32];
@@ -375,7 +385,7 @@ __global__ void __launch_bounds__(THREADS) k_diag(Planes P, Red R)
     if (t < (long long)T)
         for (int a = 0; a < c; a++)
         {
-            const double x = V.stencil[(size_t)(a * c + a) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)];
+            const double x = sten<TS>(V, (size_t)(a * c + a) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h));
             v[0] += x;
             v[1] = x < v[1] ? x : v[1];
             v[2] = x > v[2] ? x : v[2];
@@ -468,7 +478,7 @@ __device__ __forceinline__ void apply_precond(const float* minv, const double* r
 
 // y_t = (H_tt + lambda I) x_t + sum of the owned slots' blocks times the forward neighbours + the transposes of the
 // backward neighbours' blocks (src/solve_level1.cu:781-828), in the reference's order of accumulation.
-template <int C>
+template <int C, typename TS>
 __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long long t, double lambda, const double* x,
                                               double* acc)
 {
@@ -482,7 +492,7 @@ __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long
         double s = lambda * xt[i];
 #pragma unroll
         for (int j = 0; j < C; j++)
-            s += V.stencil[(size_t)(i * C + j) * T + sp] * xt[j];
+            s += sten<TS>(V, (size_t)(i * C + j) * T + sp) * xt[j];
         acc[i] = s;
     }
     // Every neighbour's loads are issued whether or not the neighbour exists (from a clamped, in-range texel), and a
@@ -502,7 +512,7 @@ __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long
 #pragma unroll
             for (int j = 0; j < C; j++)
             {
-                const double e = V.stencil[(size_t)(slot * cc + i * C + j) * T + sp] * xn[j];
+                const double e = sten<TS>(V, (size_t)(slot * cc + i * C + j) * T + sp) * xn[j];
                 acc[i] += fwd ? e : -0.0;
             }
         const int bx = tx - dx, by = ty - dy;
@@ -515,12 +525,13 @@ __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long
 #pragma unroll
             for (int j = 0; j < C; j++)
             {
-                const double e = V.stencil[(size_t)(slot * cc + j * C + i) * T + np] * xb[j];
+                const double e = sten<TS>(V, (size_t)(slot * cc + j * C + i) * T + np) * xb[j];
                 acc[i] += bwd ? e : -0.0;
             }
     }
 }
 
+template <typename TS>
 __global__ void __launch_bounds__(THREADS) k_precondition_init(Planes P, Red R)
 {
     __shared__ double sh[2 * 32];
@@ -538,7 +549,7 @@ __global__ void __launch_bounds__(THREADS) k_precondition_init(Planes P, Red R)
         double a[MAX_CH * MAX_CH], inv[MAX_CH * MAX_CH];
         for (int i = 0; i < c; i++)
             for (int j = 0; j < c; j++)
-                a[i * c + j] = V.stencil[(size_t)(i * c + j) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)] +
+                a[i * c + j] = sten<TS>(V, (size_t)(i * c + j) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)) +
                                (i == j ? lambda : 0.0);
         if (!invert(a, c, inv))
             for (int i = 0; i < c; i++)
@@ -592,7 +603,7 @@ __global__ void k_cg_start(Planes P, Red R)
     }
 }
 
-template <int C>
+template <int C, typename TS>
 __global__ void __launch_bounds__(THREADS) k_cg_matvec(Planes P, Red R)
 {
     __shared__ double sh[32];
@@ -610,7 +621,7 @@ __global__ void __launch_bounds__(THREADS) k_cg_matvec(Planes P, Red R)
     if (t < (long long)T)
     {
         double acc[MAX_CH];
-        stencil_apply<C>(V, T, t, s[S_LAMBDA], V.p, acc);
+        stencil_apply<C, TS>(V, T, t, s[S_LAMBDA], V.p, acc);
 #pragma unroll
         for (int i = 0; i < c; i++)
         {
@@ -860,7 +871,7 @@ struct SweepArgs
     unsigned int* moved;   // [plane]
 };
 
-template <int C>
+template <int C, typename TS>
 __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
 {
     const long long base = (long long)blockIdx.x * blockDim.x;
@@ -896,7 +907,7 @@ __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
 #pragma unroll
             for (int j = 0; j < c; j++)
             {
-                const double e = V.stencil[(size_t)(slot * cc + i * c + j) * T + sp] * xn[j];
+                const double e = sten<TS>(V, (size_t)(slot * cc + i * c + j) * T + sp) * xn[j];
                 nb[i] += fwd ? e : -0.0;
             }
         const int bx = tx - dx, by = ty - dy;
@@ -909,7 +920,7 @@ __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
 #pragma unroll
             for (int j = 0; j < c; j++)
             {
-                const double e = V.stencil[(size_t)(slot * cc + j * c + i) * T + np] * xb[j];
+                const double e = sten<TS>(V, (size_t)(slot * cc + j * c + i) * T + np) * xb[j];
                 nb[i] += bwd ? e : -0.0;
             }
     }
@@ -919,14 +930,14 @@ __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
     {
         const size_t idx = t * c + q;
         const float l = A.lo[q], span = A.hi[q] - A.lo[q];
-        const double a = V.stencil[(size_t)(q * c + q) * T + sp] + lambda;
+        const double a = sten<TS>(V, (size_t)(q * c + q) * T + sp) + lambda;
         if (!(a > 0.0) || !(span > 0.0f))
             continue;
         double rest = nb[q];
 #pragma unroll
         for (int j = 0; j < c; j++)
             if (j != q)
-                rest += V.stencil[(size_t)(q * c + j) * T + sp] * V.x[t * c + j];
+                rest += sten<TS>(V, (size_t)(q * c + j) * T + sp) * V.x[t * c + j];
         const double b = V.grad[idx] + rest;
         const double want = (double)V.prev[idx] - b / a;
         const int kk = grid_index(l, A.hi[q], A.bits, (float)want);
@@ -975,7 +986,7 @@ static Red red_for(nntc_b200_device* d, const Planes& P)
 }
 
 int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texels, int nmono, const double* mono,
-                   int slots);
+                   int slots, bool f32);
 int matvec_free(nntc_b200_device* d, const Planes& P, double* partial, int level0);
 
 // diag_only: the gradient and the diagonal blocks (slot 0) alone, what the matrix-free conjugate gradients of the
@@ -996,8 +1007,11 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
     const size_t shared = (size_t)SLOTS * nmono * ASM_THREADS * sizeof(double);
     AsmArgs A{ d->weights, d->bias, d->cw, d->mono[level0], nmono };
     NB_TRY(ktimer_begin(d, level0 ? NNTC_B200_K_ASSEMBLE0 : NNTC_B200_K_ASSEMBLE1));
-    if (diag_only || (!d->reference_shaped_assembly && k <= 4))
-        NB_TRY(assemble_split(d, k, level0, P, nmono, mono.data(), diag_only ? 1 : SLOTS));
+    const bool split = diag_only || (!d->reference_shaped_assembly && k <= 4);
+    // the adjoint form stores the stencil in FP32 (the split form only; the reference-shaped kernel is FP64)
+    d->sten_f32[level0] = split && d->mixed_stencil != 0;
+    if (split)
+        NB_TRY(assemble_split(d, k, level0, P, nmono, mono.data(), diag_only ? 1 : SLOTS, d->sten_f32[level0]));
     else if (level0)
     {
         NB_CUDA(cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
@@ -1013,7 +1027,10 @@ int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge,
         NB_LAUNCHED();
     const Red R = red_for(d, P);
     const int tblocks = (int)(P.start[P.n] / THREADS);
-    k_diag<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    if (d->sten_f32[level0])
+        k_diag<float><<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    else
+        k_diag<double><<<tblocks, THREADS, 0, d->stream>>>(P, R);
     NB_LAUNCHED();
     k_diag_reduce<<<P.n, 32, 0, d->stream>>>(P, R, ridge);
     NB_LAUNCHED();
@@ -1052,7 +1069,10 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     Planes P = texel_planes(d, level0, k);
     const Red R = red_for(d, P);
     const int tblocks = (int)(P.start[P.n] / THREADS);
-    k_precondition_init<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    if (d->sten_f32[level0])
+        k_precondition_init<float><<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    else
+        k_precondition_init<double><<<tblocks, THREADS, 0, d->stream>>>(P, R);
     NB_LAUNCHED();
     k_cg_start<<<P.n, 32, 0, d->stream>>>(P, R);
     NB_LAUNCHED();
@@ -1066,13 +1086,23 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
             NB_TRY(matvec_free(d, P, R.partial, level0));
         else
         {
-            switch (P.c)
+#define NB_MATVEC(TS)                                                                                                 \
+    switch (P.c)                                                                                                      \
+    {                                                                                                                 \
+    case 1: k_cg_matvec<1, TS><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;                                      \
+    case 2: k_cg_matvec<2, TS><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;                                      \
+    case 3: k_cg_matvec<3, TS><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;                                      \
+    default: k_cg_matvec<4, TS><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;                                     \
+    }
+            if (d->sten_f32[level0])
             {
-            case 1: k_cg_matvec<1><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
-            case 2: k_cg_matvec<2><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
-            case 3: k_cg_matvec<3><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
-            default: k_cg_matvec<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
+                NB_MATVEC(float)
             }
+            else
+            {
+                NB_MATVEC(double)
+            }
+#undef NB_MATVEC
             NB_LAUNCHED();
         }
         NB_TRY(ktimer_end(d));
@@ -1163,13 +1193,23 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
             SweepArgs A{ d->scalars, level0 ? d->lo0 : d->lo1, level0 ? d->hi0 : d->hi1, bits, cx, cy, d->counters + CNT_SWEEP };
             NB_TRY(ktimer_begin(d, NNTC_B200_K_SWEEP));
             const int sblocks = (int)(C.start[C.n] / THREADS);
-            switch (C.c)
+#define NB_SWEEP(TS)                                                                                                  \
+    switch (C.c)                                                                                                      \
+    {                                                                                                                 \
+    case 1: k_quant_sweep<1, TS><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;                                    \
+    case 2: k_quant_sweep<2, TS><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;                                    \
+    case 3: k_quant_sweep<3, TS><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;                                    \
+    default: k_quant_sweep<4, TS><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;                                   \
+    }
+            if (d->sten_f32[level0])
             {
-            case 1: k_quant_sweep<1><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
-            case 2: k_quant_sweep<2><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
-            case 3: k_quant_sweep<3><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
-            default: k_quant_sweep<4><<<sblocks, THREADS, 0, d->stream>>>(C, A); break;
+                NB_SWEEP(float)
             }
+            else
+            {
+                NB_SWEEP(double)
+            }
+#undef NB_SWEEP
             NB_TRY(ktimer_end(d));
             NB_LAUNCHED();
         }
@@ -1203,7 +1243,6 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     return NNTC_B200_OK;
 }
 
-// Block (c')'s assembly alone with no ridge, the correction measured from the plane as it stands (for refine_bc).
 // The gradient, the diagonal blocks and the preconditioned descent direction of one latent at its current plane:
 // grad, z = -(H_tt + lambda I)^-1 grad texel by texel, prev = v (what the joint pass steps from).
 int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0)
@@ -1212,15 +1251,27 @@ int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, doub
     Planes P = texel_planes(d, level0, k);
     const Red R = red_for(d, P);
     const int tblocks = (int)(P.start[P.n] / THREADS);
-    k_precondition_init<<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    if (d->sten_f32[level0])
+        k_precondition_init<float><<<tblocks, THREADS, 0, d->stream>>>(P, R);
+    else
+        k_precondition_init<double><<<tblocks, THREADS, 0, d->stream>>>(P, R);
     NB_LAUNCHED();
     k_snapshot<<<tblocks, THREADS, 0, d->stream>>>(P);
     NB_LAUNCHED();
     return NNTC_B200_OK;
 }
 
+// Block (c')'s assembly alone with no ridge, the correction measured from the plane as it stands (for refine_bc). The
+// refinement's decisions are the reference's on an FP64 stencil, so this assembly is FP64 in either form.
 int assemble_for_refine(nntc_b200_device* d, const nntc_b200_model* m, int k, double* ms)
 {
+    struct Fp64Scope
+    {
+        nntc_b200_device* d;
+        int was;
+        ~Fp64Scope() { d->mixed_stencil = was; }
+    } fp64{ d, d->mixed_stencil };
+    d->mixed_stencil = 0;
     NB_TRY(block_begin(d));
     NB_TRY(assemble(d, m, k, 0.0, 1));
     Planes P = texel_planes(d, 1, k);
@@ -1256,6 +1307,11 @@ int nntc_b200_set_option(nntc_b200_device* d, int option, int value)
     if (option == NNTC_B200_OPT_MIXED_OBJECTIVE)
     {
         d->mixed_objective = value != 0;
+        return NNTC_B200_OK;
+    }
+    if (option == NNTC_B200_OPT_FP32_STENCIL)
+    {
+        d->mixed_stencil = value != 0;
         return NNTC_B200_OK;
     }
     set_error(NNTC_B200_ERR_ARG, "no such option");
