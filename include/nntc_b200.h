@@ -273,12 +273,14 @@ typedef struct nntc_b200_encode_args
     int bc_outer;          /* --bc-outer 2 */
     float luma[3];         /* 0.299, 0.587, 0.114 */
     /* 0: the plain form, the reference's arithmetic (FP64 stencils and sums). 1: the adjoint + mixed-precision form:
-     * block (a)'s sums on the tensor cores (NNTC_B200_OPT_MIXED_PRECISION_GRAM), the conjugate gradients matrix-free
-     * in FP32 (NNTC_B200_OPT_ADJOINT_CG), the objective's decode in FP32 (NNTC_B200_OPT_MIXED_OBJECTIVE), the
-     * stencils of the quantised sweeps in FP32 (NNTC_B200_OPT_FP32_STENCIL), and after
-     * the repack passes one joint latent / decoder pass (bc8): a step
-     * of both latents along their preconditioned objective gradient with the decoder re-solved, the best of three
-     * step lengths, re-packed and refined, kept only when the shipped E falls. Has no counterpart in the reference. */
+     * block (a)'s sums on the tensor cores (NNTC_B200_OPT_MIXED_PRECISION_GRAM), the objective's decode in FP32
+     * (NNTC_B200_OPT_MIXED_OBJECTIVE), the stencils of blocks (b) and (c') assembled and applied in FP32
+     * (NNTC_B200_OPT_FP32_STENCIL; the conjugate gradients then stop at 1e-6 of the right-hand side), and after the
+     * repack passes one joint latent / decoder pass (bc8) along the objective's gradient from the decode's adjoint: a
+     * step of both latents along their preconditioned gradients with the decoder re-solved, the best of three step
+     * lengths, re-packed and refined, kept only when the shipped E falls. The matrix-free products of the conjugate
+     * gradients (NNTC_B200_OPT_ADJOINT_CG) are not part of it: on the B200 they cost several times an FP32 stencil
+     * product. Has no counterpart in the reference. */
     int form;
 } nntc_b200_encode_args;
 

@@ -194,8 +194,10 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     } form_scope{ d, d->mixed_gram, d->adjoint_cg, d->mixed_objective, d->mixed_stencil };
     if (a->form == 1)
     {
+        // the conjugate gradients run on the FP32 stencil: their matrix-free products (NNTC_B200_OPT_ADJOINT_CG)
+        // measured several times slower per product on the B200 than reading the assembled FP32 stencil
         d->mixed_gram = 1;
-        d->adjoint_cg = 1;
+        d->adjoint_cg = 0;
         d->mixed_objective = 1;
         d->mixed_stencil = 1;
     }

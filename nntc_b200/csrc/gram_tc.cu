@@ -177,9 +177,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v)
 __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, TcArgs A)
 {
     extern __shared__ __align__(128) unsigned char tg_sh[];
-    unsigned char* tiles = tg_sh;                                             // TG_KSTEPS tiles, 32 KB
-    float* rows = reinterpret_cast<float*>(tg_sh + TG_KSTEPS * TG_TILE_BYTES);   // [site][TG_ROW]
-    __shared__ uint64_t mbar;
+    // two operand buffers: the MMAs of one stage read one while the threads build the next stage's into the other
+    unsigned char* tiles = tg_sh;                                                       // 2 x TG_KSTEPS tiles, 64 KB
+    float* rows = reinterpret_cast<float*>(tg_sh + 2 * TG_KSTEPS * TG_TILE_BYTES);     // [site][TG_ROW]
+    __shared__ uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
 
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
     if (work)
     {
         // the zero rows 96..127 of every tile, once; the other rows are rewritten every stage
-        for (int i = tid; i < TG_KSTEPS * TG_TILE_BYTES / 16; i += TG_THREADS)
+        for (int i = tid; i < 2 * TG_KSTEPS * TG_TILE_BYTES / 16; i += TG_THREADS)
             reinterpret_cast<uint4*>(tiles)[i] = make_uint4(0u, 0u, 0u, 0u);
         if (warp == 0)
         {
@@ -212,7 +213,8 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
         }
         if (tid == 0)
         {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[0])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[1])) : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             failed = 0;
         }
@@ -222,15 +224,32 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
         const uint32_t tmem = tmem_base;
         const uint32_t tiles_addr = smem_addr(tiles);
         constexpr uint32_t idesc = umma_idesc_bf16(128, 96);
-        uint32_t phase = 0;
-        int in_batch = 0;
+        // per buffer: the parity of its next completion, and whether a commit on it is still unwaited (every thread
+        // keeps the same copy: all take the same branches)
+        uint32_t ph[2] = { 0u, 0u };
+        bool pending[2] = { false, false };
+        auto settle = [&](int x) {
+            if (!pending[x])
+                return;
+            if (!mbar_wait(&mbar[x], ph[x]))
+                failed = 1;
+            ph[x] ^= 1u;
+            pending[x] = false;
+        };
+        int in_batch = 0, stage = 0;
 
-        for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
+        for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x, stage++)
         {
-            // 1. this thread's site row, in float
+            const int bsel = stage & 1;
+            unsigned char* tb = tiles + (size_t)bsel * TG_KSTEPS * TG_TILE_BYTES;
+            // 1. this thread's site row, in float (the MMAs of the previous stage run meanwhile)
             site_row(P, V, chunk * TG_SITES + tid, sites, rows + tid * TG_ROW);
+            // 2. the buffer's previous MMAs (two stages back) are done before it is overwritten
+            settle(bsel);
             __syncthreads();
-            // 2. the operand tiles: item (column f, 8-site group g) packs 8 sites of column f into 16 bytes, hi into
+            if (failed)
+                break;
+            // 3. the operand tiles: item (column f, 8-site group g) packs 8 sites of column f into 16 bytes, hi into
             //    row f and lo into row 48 + f
             for (int it = tid; it < 48 * (TG_SITES / 8); it += TG_THREADS)
             {
@@ -247,20 +266,20 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
                     lo[q / 2] = pack_bf16x2(l0, l1);
                 }
                 const int step = g / 2, k = (g & 1) * 8;
-                *reinterpret_cast<uint4*>(tiles + tile_offset(step, f, k)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                *reinterpret_cast<uint4*>(tiles + tile_offset(step, 48 + f, k)) =
-                    make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                *reinterpret_cast<uint4*>(tb + tile_offset(step, f, k)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<uint4*>(tb + tile_offset(step, 48 + f, k)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
             }
-            // generic-proxy stores become visible to the tensor core's async proxy
+            // generic-proxy stores become visible to the tensor core's async proxy; the rows are free again
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // 3. one thread issues the stage's MMAs and commits them to the barrier
+            // 4. one thread issues the stage's MMAs and commits them to the buffer's barrier; nobody waits here
             if (tid == 0)
             {
+                const uint32_t base = tiles_addr + (uint32_t)bsel * TG_KSTEPS * TG_TILE_BYTES;
                 for (int s = 0; s < TG_KSTEPS; s++)
                 {
-                    const uint64_t desc = umma_desc(tiles_addr + (uint32_t)s * TG_TILE_BYTES, 128, 256);
+                    const uint64_t desc = umma_desc(base + (uint32_t)s * TG_TILE_BYTES, 128, 256);
                     const uint32_t accumulate = (in_batch > 0 || s > 0) ? 1u : 0u;
                     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
@@ -268,21 +287,20 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
                                  : "memory");
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_addr(&mbar))
+                                 smem_addr(&mbar[bsel]))
                              : "memory");
             }
-            // 4. every thread waits for the MMAs (the tiles and rows are reused next stage)
-            if (!mbar_wait(&mbar, phase))
-                failed = 1;
-            phase ^= 1u;
-            __syncthreads();
-            if (failed)
-                break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            pending[bsel] = true;
             const bool last = chunk + gridDim.x >= chunks;
             if (++in_batch == TG_STAGES_PER_BATCH || last)
             {
-                // 5. the batch's FP32 sums into FP64: row r of D, columns j (hi part) and 48 + j (lo part)
+                // 5. the batch's MMAs done, its FP32 sums into FP64: row r of D, columns j (hi) and 48 + j (lo)
+                settle(0);
+                settle(1);
+                __syncthreads();
+                if (failed)
+                    break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 if (warp < 3)
                 {
                     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
@@ -315,7 +333,10 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
         {
             if (tid == 0)
                 atomicOr(A.status, 1u);
-            mbar_wait(&mbar, phase);   // bounded: whatever the tensor core still holds of this CTA's work
+            // bounded: whatever the tensor core still holds of this CTA's work
+            for (int x = 0; x < 2; x++)
+                if (pending[x])
+                    mbar_wait(&mbar[x], ph[x]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
@@ -349,7 +370,7 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
 
 size_t ls_tc_shared_bytes()
 {
-    const size_t stage = (size_t)TG_KSTEPS * TG_TILE_BYTES + (size_t)TG_SITES * TG_ROW * sizeof(float);
+    const size_t stage = (size_t)2 * TG_KSTEPS * TG_TILE_BYTES + (size_t)TG_SITES * TG_ROW * sizeof(float);
     const size_t sums = (size_t)96 * 49 * sizeof(double);
     return stage > sums ? stage : sums;
 }

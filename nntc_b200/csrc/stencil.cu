@@ -1116,7 +1116,8 @@ int solve_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
         default: k_cg_update<4><<<tblocks, THREADS, 0, d->stream>>>(P, R); break;
         }
         NB_LAUNCHED();
-        k_cg_beta<<<P.n, 32, 0, d->stream>>>(P, R, it, active + (it % CG_PROBE), adjoint ? CG_TOL_FP32 : CG_TOL);
+        k_cg_beta<<<P.n, 32, 0, d->stream>>>(P, R, it, active + (it % CG_PROBE),
+                                             adjoint || d->sten_f32[level0] ? CG_TOL_FP32 : CG_TOL);
         NB_LAUNCHED();
         k_cg_direction<<<tblocks, THREADS, 0, d->stream>>>(P, R);
         NB_LAUNCHED();
