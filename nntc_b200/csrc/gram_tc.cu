@@ -16,8 +16,8 @@
 // entry, which k_ls_reduce folds in block order as it does for the FP64 form. Deterministic: the tensor core's sums of
 // a batch are a fixed function of the tile, the rest is fixed-order FP64.
 //
-// The tensor-core plumbing, all by inline PTX: tcgen05.alloc / dealloc of 128 TMEM columns per CTA (at most three CTAs
-// fit an SM by shared memory, so an allocation never waits on another CTA), shared-memory matrix descriptors of the
+// The tensor-core plumbing, all by inline PTX: tcgen05.alloc / dealloc of 128 TMEM columns per CTA (three CTAs per SM
+// by registers and shared memory, 384 of the 512 columns, so an allocation never waits on another CTA), shared-memory matrix descriptors of the
 // no-swizzle K-major canonical layout (8-row x 16-byte core matrices, LBO = the K-neighbour's offset, SBO = the next
 // eight rows'), tcgen05.mma.cta_group::1.kind::f16 issued by one thread, tcgen05.commit to an mbarrier, tcgen05.ld of
 // 32 lanes x 32 columns per warp. No TMA, no multicast, no cluster: the operands are built in shared memory by the
@@ -40,6 +40,9 @@ constexpr int TG_STAGES_PER_BATCH = 2;    // FP32 accumulation spans 256 sites
 constexpr int TG_ROW = 57;                // floats per staged site row (odd: conflict-free column reads)
 constexpr int TG_TILE_BYTES = 128 * 16 * 2;   // one K-step operand tile: 128 rows x 16 bf16
 constexpr int TG_TMEM_COLS = 128;         // allocation (power of two >= 96)
+constexpr int TG_BUFFERS = 1;             // operand buffers: one stage's MMAs run while the next stage's site rows
+                                          // are formed; a second buffer (the tile build overlapping too) measured no
+                                          // faster and costs the third CTA per SM
 constexpr uint32_t TG_WAIT_LIMIT = 1u << 26;
 
 struct TcArgs
@@ -174,12 +177,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v)
                  : "r"(taddr));
 }
 
-__global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, TcArgs A)
+__global__ void __launch_bounds__(TG_THREADS, 3) k_ls_accumulate_tc(Planes P, TcArgs A)
 {
     extern __shared__ __align__(128) unsigned char tg_sh[];
-    // two operand buffers: the MMAs of one stage read one while the threads build the next stage's into the other
-    unsigned char* tiles = tg_sh;                                                       // 2 x TG_KSTEPS tiles, 64 KB
-    float* rows = reinterpret_cast<float*>(tg_sh + 2 * TG_KSTEPS * TG_TILE_BYTES);     // [site][TG_ROW]
+    // the operand buffers (TG_BUFFERS x TG_KSTEPS tiles of 4 KB), then the staged site rows [site][TG_ROW]
+    unsigned char* tiles = tg_sh;
+    float* rows = reinterpret_cast<float*>(tg_sh + TG_BUFFERS * TG_KSTEPS * TG_TILE_BYTES);
     __shared__ uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
     if (work)
     {
         // the zero rows 96..127 of every tile, once; the other rows are rewritten every stage
-        for (int i = tid; i < 2 * TG_KSTEPS * TG_TILE_BYTES / 16; i += TG_THREADS)
+        for (int i = tid; i < TG_BUFFERS * TG_KSTEPS * TG_TILE_BYTES / 16; i += TG_THREADS)
             reinterpret_cast<uint4*>(tiles)[i] = make_uint4(0u, 0u, 0u, 0u);
         if (warp == 0)
         {
@@ -240,11 +243,11 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
 
         for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x, stage++)
         {
-            const int bsel = stage & 1;
+            const int bsel = stage % TG_BUFFERS;
             unsigned char* tb = tiles + (size_t)bsel * TG_KSTEPS * TG_TILE_BYTES;
             // 1. this thread's site row, in float (the MMAs of the previous stage run meanwhile)
             site_row(P, V, chunk * TG_SITES + tid, sites, rows + tid * TG_ROW);
-            // 2. the buffer's previous MMAs (two stages back) are done before it is overwritten
+            // 2. the buffer's previous MMAs are done before it is overwritten
             settle(bsel);
             __syncthreads();
             if (failed)
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(TG_THREADS, 2) k_ls_accumulate_tc(Planes P, Tc
 
 size_t ls_tc_shared_bytes()
 {
-    const size_t stage = (size_t)2 * TG_KSTEPS * TG_TILE_BYTES + (size_t)TG_SITES * TG_ROW * sizeof(float);
+    const size_t stage = (size_t)TG_BUFFERS * TG_KSTEPS * TG_TILE_BYTES + (size_t)TG_SITES * TG_ROW * sizeof(float);
     const size_t sums = (size_t)96 * 49 * sizeof(double);
     return stage > sums ? stage : sums;
 }
