@@ -1,8 +1,8 @@
 """Whole encodes of the two forms on a B200, and parity at the larger configurations.
 
-- The adjoint + mixed-precision form (tensor-core normal equations, matrix-free FP32 conjugate gradients, FP32
-  objective, the joint pass) against the plain form on the same material: per-texture PSNR within 0.05 dB; the joint
-  pass never leaves the shipped E above where it started.
+- The adjoint + mixed-precision form (tensor-core normal equations, FP32 stencils and FP32-product conjugate
+  gradients, FP32 objective, the joint pass along the adjoint's gradient) against the plain form on the same material:
+  per-texture PSNR within 0.05 dB; the joint pass never leaves the shipped E above where it started.
 - The 4 x 1024 x 1024 material (c0 2, c1 4): the plain form against the reference's own CPU encoder
   (oracle/_ref/nntc_encode_cpu), per-texture PSNR within 0.05 dB.
 - The 4 x 2048 x 1024 material (c0 4, c1 4): both forms against the reference's own CUDA encoder
