@@ -88,13 +88,12 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
     NB_TRY(objective(e));
     double best_e = e.e;
     float best = 0.0f;
+    // the step lengths tried with the decoder held (E alone decides among them); the decoder is re-solved once, at
+    // the step taken
     for (float alpha = 1.0f; alpha >= 0.25f; alpha *= 0.5f)
     {
-        *m = keep_m;
-        NB_TRY(nntc_b200_upload_decoder(d, m));
         NB_TRY(nb::joint_apply(d, m, k, 0, alpha));
         NB_TRY(nb::joint_apply(d, m, k, 1, alpha));
-        NB_TRY(block_a());
         NB_TRY(objective(e));
         if (e.e < best_e)
         {
