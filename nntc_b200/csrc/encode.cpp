@@ -349,7 +349,10 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     {
         nntc_b200_objective ea{}, eb{}, ec{};
         NB_TRY(block_a());
-        NB_TRY(objective(ea));
+        // E after blocks (a) and (b) is the reference's report (src/main.cpp's per-block lines) and decides nothing;
+        // the adjoint form leaves it out, the plain form keeps the reference's passes
+        if (a->form == 0)
+            NB_TRY(objective(ea));
         if (a->q1_start > 0 && round >= a->q1_start && !frozen)
         {
             NB_TRY(nntc_b200_freeze_level1_grid(d, m, a->range_pct, nullptr));
@@ -370,7 +373,8 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             delta2 += lr[(size_t)p].delta2;
             plane2 += lr[(size_t)p].plane2;
         }
-        NB_TRY(objective(eb));
+        if (a->form == 0)
+            NB_TRY(objective(eb));
         long long moved0 = 0;
         if (bc8)
         {
