@@ -228,6 +228,7 @@ def main():
     ap.add_argument("--crop", type=int, default=256, help="edge of the CPU-baseline crop")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the mixed-precision error report")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -413,6 +414,15 @@ def main():
             "pipe_peaks": pipes,
             "clocks": clocks.summary(),
         }
+        if world == 1 and not args.no_precision:
+            # the adjoint form's errors against the FP64 form at the state an adjoint-form encode ships
+            from nntc_b200.session import Session
+            with Session(mat) as s:
+                s.encode(encode_args(L, "adjoint"))
+                line["precision_vs_fp64"] = {k: float(f"{v:.3g}") for k, v in s.precision_report(mat.k).items()}
+                line["precision_vs_fp64"]["what"] = (
+                    "max relative error against the FP64 form from the same state: decoder coefficients (tensor-core "
+                    "sums vs FP64 sums, per output row), one block (b) / (c') correction (FP32 vs FP64 stencil)")
         if world == 1 and not args.no_reference_cuda:
             line["reference_cuda"] = reference_cuda(mat, os.cpu_count() or 1)
             if "psnr" in line["reference_cuda"]:

@@ -187,3 +187,70 @@ class Session:
         from . import asset
         return asset.write_asset(self.m, prefix, outputs["k1"], k0=outputs["k0"], ep=outputs["ep"],
                                  sel=outputs["sel"], source_size=source_size, json_path=json_path)
+
+    def precision_report(self, k=4):
+        """The adjoint form's mixed precision against the FP64 form, from this session's current state (both latents,
+        their indices and the decoder are put back afterwards):
+
+        - `decoder`: the decoder solved from the tensor-core normal equations (BF16 hi + lo, FP32 accumulation)
+          against the one solved from the FP64 sums, the largest difference of a coefficient relative to the largest
+          coefficient of its output row;
+        - `level1`, `level0`: one block (b) / block (c') solve with the FP32 stencil against the FP64 stencil, the
+          largest difference of the correction relative to the correction's largest entry, over every plane (level 0
+          under bc8 only)."""
+        L = lib()
+        m = self.m
+        n = m.nplanes
+        v0 = [self.get_v0(i) for i in range(n)]
+        v1 = [self.get_v1(i) for i in range(n)]
+        k0 = [self.get_k0(i) for i in range(n)]
+        k1 = [self.get_k1(i) for i in range(n)]
+        saved = abi.Model.from_buffer_copy(m)
+
+        def restore():
+            C.memmove(C.addressof(m), C.addressof(saved), C.sizeof(m))
+            check(L.nntc_b200_upload_decoder(self.d, C.byref(m)), "decoder")
+            check(L.nntc_b200_upload_grids(self.d, C.byref(m)), "grids")
+            for i in range(n):
+                self.set_planes(i, v0[i], v1[i])
+                L.nntc_b200_level0_upload_indices(self.d, i, k0[i].ctypes.data_as(C.POINTER(C.c_uint8)), k0[i].size)
+                L.nntc_b200_level1_upload_indices(self.d, i, k1[i].ctypes.data_as(C.POINTER(C.c_uint8)), k1[i].size)
+
+        def options(value):
+            for opt in (abi.OPT_MIXED_PRECISION_GRAM, abi.OPT_FP32_STENCIL):
+                check(L.nntc_b200_set_option(self.d, opt, value), "option")
+
+        out = {}
+        dec = []
+        for mixed in (0, 1):
+            restore()
+            options(mixed)
+            m.has_decoder = 0
+            self.solve_decoder(k)
+            w, b = self.decoder()
+            dec.append(np.concatenate([w, b[:, None]], axis=1).astype(np.float64))
+        out["decoder"] = float((np.abs(dec[1] - dec[0]) / np.abs(dec[0]).max(axis=1, keepdims=True)).max())
+        for level0 in ((False, True) if m.l0_bc8 else (False,)):
+            xs = []
+            for mixed in (0, 1):
+                restore()
+                options(mixed)
+                self.block(level0, k=k)
+                per = []
+                for i in range(n):
+                    c = m.c0 if level0 else m.c1
+                    t = self.n0(i) if level0 else self.n1(i)
+                    x = np.zeros(t * c)
+                    check(L.nntc_b200_probe_workspace(self.d, i, 1 if level0 else 0, None, None, None,
+                                                      x.ctypes.data_as(C.POINTER(C.c_double)), None), "workspace")
+                    per.append(x)
+                xs.append(per)
+            worst = 0.0
+            for x64, x32 in zip(xs[0], xs[1]):
+                scale = np.abs(x64).max()
+                if scale > 0:
+                    worst = max(worst, float(np.abs(x32 - x64).max() / scale))
+            out["level0" if level0 else "level1"] = worst
+        options(0)
+        restore()
+        return out

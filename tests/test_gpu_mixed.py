@@ -54,3 +54,16 @@ def test_tensor_core_normal_equations_vs_fp64(textures, c0, c1, w, h, k):
     row_scale = np.abs(x64).max(axis=1, keepdims=True)
     rel = np.abs(x_tc - x64) / row_scale
     assert rel.max() <= 1e-4, rel.max()
+
+
+def test_precision_report_against_fp64():
+    """The adjoint form's errors against the FP64 form after an encode of a small material (c0 = c1 = 4): the decoder
+    from the tensor-core sums and one block (b) and (c') solve on the FP32 stencil, each within 1e-4 relative."""
+    mat = materials.small(31, 96, 80, textures=4, c0=4, c1=4)
+    with Session(mat) as s:
+        a = abi.EncodeArgs()
+        lib().nntc_b200_encode_defaults(a)
+        a.form = 1
+        s.encode(a)
+        rep = s.precision_report()
+    assert rep["decoder"] <= 1e-4 and rep["level1"] <= 1e-4 and rep["level0"] <= 1e-4, rep
