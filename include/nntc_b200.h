@@ -294,7 +294,8 @@ typedef struct nntc_b200_encode_result
     double psnr[6];        /* per texture: 8-bit decode at the base plane's texel centres vs the source bytes */
     double ms_a, ms_b, ms_c, ms_e, ms_pack, ms_refine, ms_total;   /* CUDA-event spans of each kind of block */
     long long objective_passes;
-    int joint_taken;       /* form 1: the joint pass was kept (the shipped E fell) */
+    int joint_taken;       /* form 1: 1 the joint pass was kept (the shipped E fell, no texture's base PSNR fell by
+                              more than 0.01 dB), 0 refused (E did not fall), -1 refused by the PSNR guard */
     double e_before_joint; /* form 1: the shipped E the joint pass started from (0 when it did not run) */
     double e_joint;        /* form 1: the shipped E the joint pass reached, kept or not (0 when it did not run) */
     double ms_joint;       /* form 1: the joint pass's span */

@@ -55,15 +55,22 @@ namespace nb
 {
 int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0);
 int joint_apply(nntc_b200_device* d, const nntc_b200_model* m, int k, int level0, float alpha);
+int psnr_base(nntc_b200_device* d, const nntc_b200_model* m, double* psnr);
 }
 
 namespace
 {
 
+constexpr double JOINT_PSNR_SLACK = 0.01;   // dB a texture's base-level PSNR may lose to the joint pass
+
 // The adjoint form's joint pass (bc8, after the repack passes; the method is described in joint.cu): both latents step
 // along their preconditioned objective gradients by the best of alpha in {1, 1/2, 1/4} (snapped onto their grids, the
-// decoder re-solved at every trial), the step is re-packed into BC blocks and refined, and the whole pass is kept only
-// when the shipped E falls below e_ship; otherwise every part of the state is restored exactly.
+// decoder held), the decoder is re-solved at the step taken, the step is re-packed into BC blocks and refined, and the
+// whole pass is kept only when the shipped E falls below e_ship AND no texture's 8-bit PSNR at the base level falls
+// by more than JOINT_PSNR_SLACK dB; otherwise every part of the state is restored exactly. The guard exists because E
+// is one sum over every texture: a step that lowers it can move error from the textures with the most of it onto
+// the nearly exact ones (a binary metalness map loses decibels to a handful of texels that cross an 8-bit rounding
+// boundary while E barely moves).
 template <class Obj, class BlockA>
 int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_args* a, int k,
                const double* per_site, Obj objective, BlockA block_a, double& e_ship, nntc_b200_encode_result* r)
@@ -74,6 +81,8 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
     NB_CUDA(cudaEventCreate(&j1));
     NB_CUDA(cudaEventRecord(j0, d->stream));
     r->e_before_joint = e_ship;
+    double psnr_before[6] = {};
+    NB_TRY(nb::psnr_base(d, m, psnr_before));
     NB_TRY(snapshot(d, true));
     const nntc_b200_model keep_m = *m;
     auto restore = [&]() -> int {
@@ -119,13 +128,21 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
         r->ms_refine += ms;
         NB_TRY(objective(e));
         r->e_joint = e.e;
-        if (e.e < e_ship)
+        double psnr_after[6] = {};
+        NB_TRY(nb::psnr_base(d, m, psnr_after));
+        bool guard = true;
+        for (int t = 0; t < m->textures && t < 6; t++)
+            guard = guard && psnr_after[t] >= psnr_before[t] - JOINT_PSNR_SLACK;
+        if (e.e < e_ship && guard)
         {
             e_ship = e.e;
             r->joint_taken = 1;
         }
         else
+        {
+            r->joint_taken = e.e < e_ship ? -1 : 0;
             st = restore();
+        }
     }
     NB_CUDA(cudaEventRecord(j1, d->stream));
     NB_CUDA(cudaEventSynchronize(j1));
@@ -142,7 +159,6 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
 namespace nb
 {
 int channel_copies(nntc_b200_device* d, std::vector<unsigned char>& same);
-int psnr_base(nntc_b200_device* d, const nntc_b200_model* m, double* psnr);
 }
 
 using namespace nb;

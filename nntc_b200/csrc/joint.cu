@@ -14,9 +14,10 @@
 // preconditioned descent directions z = -(H_tt + lambda I)^-1 dE/dv (block Jacobi, the diagonal blocks the CG uses)
 // by a step alpha in {1, 1/2, 1/4}, each snapped onto its grid; the alpha with the lowest E, if it lowers E, is taken
 // with the decoder re-solved exactly at it (block (a) is the decoder's exact step given the latents), re-packed into BC
-// blocks, refined, and kept only when the shipped E falls below the shipped E it started from; otherwise everything
-// (both latents, their indices, the BC state, the decoder and the grids) is restored exactly. The shipped E therefore
-// never rises across the pass.
+// blocks, refined, and kept only when the shipped E falls below the shipped E it started from and no texture's
+// base-level 8-bit PSNR falls by more than 0.01 dB; otherwise everything (both latents, their indices, the BC state,
+// the decoder and the grids) is restored exactly. The shipped E therefore never rises across the pass, and no texture
+// pays for another's gain.
 
 #include <cmath>
 #include <cstring>

@@ -2,7 +2,8 @@
 
 - The adjoint + mixed-precision form (tensor-core normal equations, FP32 stencils and FP32-product conjugate
   gradients, FP32 objective, the joint pass along the adjoint's gradient) against the plain form on the same material:
-  per-texture PSNR within 0.05 dB; the joint pass never leaves the shipped E above where it started.
+  per-texture PSNR within 0.05 dB; the joint pass never leaves the shipped E above where it started (it is kept only
+  when E falls and no texture's base-level PSNR falls by more than 0.01 dB).
 - The 4 x 1024 x 1024 material (c0 2, c1 4): the plain form against the reference's own CPU encoder
   (oracle/_ref/nntc_encode_cpu), per-texture PSNR within 0.05 dB.
 - The 4 x 2048 x 1024 material (c0 4, c1 4): both forms against the reference's own CUDA encoder
@@ -50,7 +51,7 @@ def test_adjoint_form_vs_plain(index):
     assert all(abs(x - y) <= 0.05 for x, y in zip(a, b)), (a, b)
     if adj.e_before_joint > 0:
         assert adj.e_ship <= adj.e_before_joint * (1 + 1e-12), (adj.e_ship, adj.e_before_joint, adj.joint_taken)
-        if adj.joint_taken:
+        if adj.joint_taken == 1:
             assert adj.e_joint < adj.e_before_joint
 
 
