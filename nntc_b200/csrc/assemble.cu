@@ -111,7 +111,9 @@ struct SiteDecoder
     float cw[MAX_NOUT];
 };
 
-template <bool LEVEL0, int NOUT>
+// MIXED (the adjoint form, whose stencil and sums are FP32): the same terms with fused multiply-adds and the gradient
+// term summed in FP32 - half the instructions of the reference's unfused float arithmetic and no FP64 work per output.
+template <bool LEVEL0, int NOUT, bool MIXED>
 __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __grid_constant__ SiteArgs A, SiteDecoder W)
 {
     const long long base = (long long)blockIdx.x * blockDim.x;
@@ -145,9 +147,15 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
     // the targets: the pixel's own source at the centre site, else the fractional site's blend from k_site_targets
     const float* tgt = j > 0 ? A.tgt + (size_t)(A.tsite0[pl] + pixel * kc + (j - 1)) * NOUT : V.src + pixel * NOUT;
     double acc[MAX_CH];
+    float accf[MAX_CH];
 #pragma unroll
     for (int a = 0; a < MAX_CH; a++)
+    {
         acc[a] = 0.0;
+        accf[a] = 0.0f;
+    }
+    // a + b c, unfused (the reference's rounding) or fused (MIXED)
+    auto madd = [](float a, float b, float c) { return MIXED ? __fmaf_rn(b, c, a) : a + b * c; };
 #pragma unroll
     for (int r = 0; r < NOUT; r++)
     {
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
 #pragma unroll
             for (int i = 0; i < MAX_CH; i++)
                 if (i < c0)
-                    out += row[4 + i] * sbar[i];
+                    out = madd(out, row[4 + i], sbar[i]);
 #pragma unroll
             for (int q = 0; q < MAX_CH; q++)
                 if (q < c1)
@@ -169,9 +177,9 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
 #pragma unroll
                     for (int i = 0; i < MAX_CH; i++)
                         if (i < c0)
-                            gg += sbar[i] * row[8 + i * 4 + q];
+                            gg = madd(gg, sbar[i], row[8 + i * 4 + q]);
                     col[q] = gg;
-                    out += gg * cbar[q];
+                    out = madd(out, gg, cbar[q]);
                 }
         }
         else
@@ -179,7 +187,7 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
 #pragma unroll
             for (int q = 0; q < MAX_CH; q++)
                 if (q < c1)
-                    out += row[q] * cbar[q];
+                    out = madd(out, row[q], cbar[q]);
 #pragma unroll
             for (int i = 0; i < MAX_CH; i++)
                 if (i < c0)
@@ -188,9 +196,9 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
 #pragma unroll
                     for (int q = 0; q < MAX_CH; q++)
                         if (q < c1)
-                            qq += cbar[q] * row[8 + i * 4 + q];
+                            qq = madd(qq, cbar[q], row[8 + i * 4 + q]);
                     col[i] = qq;
-                    out += qq * sbar[i];
+                    out = madd(out, qq, sbar[i]);
                 }
         }
         const float res = out - target;
@@ -198,7 +206,18 @@ __global__ void __launch_bounds__(SITE_THREADS) k_site_terms(Planes P, const __g
 #pragma unroll
         for (int a = 0; a < MAX_CH; a++)
             if (a < c)
-                acc[a] += (double)W.cw[r] * (double)col[a] * (double)res;
+            {
+                if (MIXED)
+                    accf[a] = __fmaf_rn(W.cw[r] * col[a], res, accf[a]);
+                else
+                    acc[a] += (double)W.cw[r] * (double)col[a] * (double)res;
+            }
+    }
+    if (MIXED)
+    {
+#pragma unroll
+        for (int a = 0; a < MAX_CH; a++)
+            acc[a] = (double)accf[a];
     }
     const int c = LEVEL0 ? c0 : c1;
     double* out_t = A.terms + (size_t)(A.site0[pl] + si) * c;
@@ -693,9 +712,16 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
 #define NB_SITES(NO)                                                                                                  \
     case NO:                                                                                                          \
         if (level0)                                                                                                   \
-            k_site_terms<true, NO><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                                 \
+        {                                                                                                             \
+            if (f32)                                                                                                  \
+                k_site_terms<true, NO, true><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                       \
+            else                                                                                                      \
+                k_site_terms<true, NO, false><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                      \
+        }                                                                                                             \
+        else if (f32)                                                                                                 \
+            k_site_terms<false, NO, true><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                          \
         else                                                                                                          \
-            k_site_terms<false, NO><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                                \
+            k_site_terms<false, NO, false><<<sblocks, SITE_THREADS, 0, d->stream>>>(S, A, W);                         \
         break;
     switch (d->nout)
     {

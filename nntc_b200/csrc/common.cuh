@@ -32,9 +32,10 @@ constexpr int SLOTS = 5;          // owned stencil blocks per texel: self, right
 constexpr int MAX_MONO = 15;      // 1 + C + C (C + 1) / 2 at C = 4
 constexpr int CG_PROBE = 4;       // the host looks at the residual every 4th iteration (src/solve_level1.cu:99)
 // The stop of conjugate gradients whose products are FP32 (the matrix-free operator, or an FP32 stencil: about 1e-7
-// relative): the recursive residual is trusted down to 1e-6 of the right-hand side, where the FP64 stencil form goes
-// on to 1e-10.
-constexpr double CG_TOL_FP32 = 1e-6;
+// relative): the recursive residual is taken down to 1e-7 of the right-hand side, where the FP64 stencil form goes
+// on to 1e-10 (at 1e-6 the correction of a converged level-0 state differed from the FP64 form's by 1.3e-4 of its
+// largest entry, above the 1e-4 the form is held to).
+constexpr double CG_TOL_FP32 = 1e-7;
 constexpr int CG_MAX_IT = 200;    // src/solve_level1.cu:1261
 constexpr double CG_TOL = 1e-10;  // src/solve_level1.cu:1257
 

@@ -18,37 +18,41 @@
 #include <vector>
 
 #include "device.cuh"
+#include "site_rows.cuh"
 
 namespace nb
 {
 
-size_t ls_tc_shared_bytes();
-int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries, cudaStream_t stream);
+int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries,
+                            const SiteTargetView& tgt, cudaStream_t stream);
+int ensure_site_targets(nntc_b200_device* d, int k, int level0);
 
 struct LsArgs
 {
     double* partial;   // [plane][entry][LS_GRID]
     int entries;
+    SiteTargetView tgt;
 };
 
 // ---- the accumulation on the FP64 tensor cores
 //
-// Z = [phi (nin) | 1 | t (nout) | 0 ...] per site, 48 columns in six blocks of eight, and every product the normal
-// equations need is an entry of the 48 x 48 Gram Z^T Z: A from its upper-left mm x mm corner, the right-hand sides
-// from the columns after it. The 18 upper block pairs (I <= J, I < 4) of the Gram are accumulated with the FP64
-// tensor-core MMA (m8n8k4: an 8x4 slice of Z_I^T times a 4x8 slice of Z_J, four sites per step, every product exact
-// in double since both factors are floats). One block stages 128 sites' rows of Z; each of its four warps
-// takes 32 of them and keeps all 18 tiles in registers over all of its chunks; the warps' tiles are added in warp
-// order and each block writes one partial per entry, folded across blocks by k_ls_reduce in block order:
-// deterministic.
+// Z = [phi | 1 | t] per site in site_z()'s fixed 48-slot layout (six blocks of eight: slots 0..24 the columns of the
+// system, 25.. the targets), and every product the normal equations need is an entry of the 48 x 48 Gram Z^T Z: A from
+// the rows and columns of phi and 1, the right-hand sides from the rows of phi and 1 against the target columns. The
+// 18 upper block pairs (I <= J, I < 4) of the Gram are accumulated with the FP64 tensor-core MMA (m8n8k4: an 8x4 slice
+// of Z_I^T times a 4x8 slice of Z_J, four sites per step, every product exact in double since both factors are
+// floats). A block takes 128 texels at a time, one per thread, and stages their rows site by site (the centre, then
+// each fractional site: every lane of a warp takes the same branch); each of its four warps multiplies 32 of the
+// staged rows and keeps all 18 tiles in registers over all of its chunks; the warps' tiles are added in warp order
+// and each block writes one partial per entry, folded across blocks by k_ls_reduce in block order: deterministic.
 
 constexpr int NE_THREADS = 128;
 constexpr int NE_WARPS = NE_THREADS / 32;
 constexpr int NE_STRIDE = 57;    // floats per staged site: 48 columns; an odd stride keeps the staging stores (one
                                  // row per lane) conflict-free, and 57 = 25 (mod 32) spreads the four sites of one
                                  // fragment load over the banks
-constexpr int NE_TILES = 18;     // block pairs I <= J of six blocks with I <= 3: the rows a < mm <= 25 the system
-                                 // reads (pairs of two target blocks are never needed)
+constexpr int NE_TILES = 18;     // block pairs I <= J of six blocks with I <= 3: the rows a < 32 the system reads
+                                 // (pairs of two target blocks are never needed)
 
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b)
 {
@@ -66,16 +70,17 @@ __host__ __device__ constexpr int tile_j(int t)
     return t < 6 ? t : (t < 11 ? t - 5 : (t < 15 ? t - 9 : (t < 18 ? t - 12 : (t < 20 ? t - 14 : 5))));
 }
 
-__global__ void __launch_bounds__(NE_THREADS, 4) k_ls_accumulate_mma(Planes P, LsArgs A)
+template <int NOUT>
+__global__ void __launch_bounds__(NE_THREADS, 4) k_ls_accumulate_mma(Planes P, const __grid_constant__ LsArgs A)
 {
     extern __shared__ double ne_sh[];
     float* sz = (float*)ne_sh;   // [site][NE_STRIDE] floats; after the chunks, the warps' tiles as doubles
     const int pl = blockIdx.y;
     const PlaneView& V = P.p[pl];
-    const int c0 = P.c0, c1 = P.c1, nin = P.nin, nout = P.nout, kc = P.kc, mm = nin + 1;
-    const int per_pixel = 1 + kc;
-    const size_t sites = (size_t)V.w0 * V.h0 * per_pixel;
-    const size_t chunks = (sites + NE_THREADS - 1) / NE_THREADS;
+    const int nin = P.nin, mm = nin + 1, kc = P.kc;
+    const long long texels = (long long)V.w0 * V.h0;
+    const long long chunks = (texels + NE_THREADS - 1) / NE_THREADS;
+    const float* tgt = A.tgt.t + (size_t)A.tgt.site0[pl] * NOUT;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double acc[NE_TILES][2];
 #pragma unroll
@@ -85,83 +90,42 @@ __global__ void __launch_bounds__(NE_THREADS, 4) k_ls_accumulate_mma(Planes P, L
         acc[t][1] = 0.0;
     }
 
-    for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
+    for (long long chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
     {
-        const size_t si = chunk * NE_THREADS + tid;
-        __syncthreads();   // the previous chunk's fragments have been read
-        float* row = sz + tid * NE_STRIDE;
-        // the site's row of Z with the solver's arithmetic (src/sample.cuh:154-178); a site outside the plane stages
-        // zeros
-        int q = 0;
-        if (si < sites)
+        const long long pixel = chunk * NE_THREADS + tid;
+        const bool valid = pixel < texels;
+        const int px = valid ? (int)(pixel % V.w0) : 0, py = valid ? (int)(pixel / V.w0) : 0;
+        for (int j = 0; j <= kc; j++)
         {
-            const size_t pixel = si / (size_t)per_pixel;
-            const int j = (int)(si % (size_t)per_pixel);
-            const int px = (int)(pixel % (size_t)V.w0), py = (int)(pixel / (size_t)V.w0);
-            float dx, dy;
-            site_offset(kc, j, px, py, dx, dy);
-            float s[MAX_CH], c[MAX_CH];
-            const Tap t1 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1);
-            blend_u<MAX_CH>(V.v1, V.w1, c1, t1, c);
-            Tap t0{};
-            float w4[4];
-            if (j == 0)
-            {
-#pragma unroll
-                for (int i = 0; i < MAX_CH; i++)
-                    if (i < c0)
-                        s[i] = __ldg(V.v0 + pixel * c0 + i);
-            }
+            float z[ZS_WIDTH];
+            if (valid)
+                site_z<NOUT>(P, V, tgt, pixel, px, py, j, z);
             else
             {
-                t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
-                blend_u<MAX_CH>(V.v0, V.w0, c0, t0, s);
-                tap_weights(t0, w4);
+#pragma unroll
+                for (int q = 0; q < ZS_WIDTH; q++)
+                    z[q] = 0.0f;
             }
+            __syncthreads();   // the previous stage's fragments have been read
+            float* row = sz + tid * NE_STRIDE;
 #pragma unroll
-            for (int jj = 0; jj < MAX_CH; jj++)
-                if (jj < c1)
-                    row[q++] = c[jj];
-#pragma unroll
-            for (int i = 0; i < MAX_CH; i++)
-                if (i < c0)
-                    row[q++] = s[i];
-#pragma unroll
-            for (int i = 0; i < MAX_CH; i++)
-#pragma unroll
-                for (int jj = 0; jj < MAX_CH; jj++)
-                    if (i < c0 && jj < c1)
-                        row[q++] = s[i] * c[jj];
-            row[q++] = 1.0f;
-            for (int r = 0; r < nout; r++)
-            {
-                float t;
-                if (j == 0)
-                    t = __ldg(V.src + pixel * nout + r);
-                else
-                    t = w4[0] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x0) * nout + r) +
-                        w4[1] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x1) * nout + r) +
-                        w4[2] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x0) * nout + r) +
-                        w4[3] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x1) * nout + r);
-                row[q++] = t;
-            }
-        }
-        for (; q < 48; q++)
-            row[q] = 0.0f;
-        __syncthreads();
-        // this warp's 32 sites, four per step
-        const float* base = sz + (size_t)(warp * 32 + (lane & 3)) * NE_STRIDE + (lane >> 2);
+            for (int q = 0; q < ZS_WIDTH; q++)
+                row[q] = z[q];
+            __syncthreads();
+            // this warp's 32 sites, four per step
+            const float* base = sz + (size_t)(warp * 32 + (lane & 3)) * NE_STRIDE + (lane >> 2);
 #pragma unroll 2
-        for (int step = 0; step < 8; step++)
-        {
-            const float* f = base + (size_t)step * 4 * NE_STRIDE;
-            double frag[6];
+            for (int step = 0; step < 8; step++)
+            {
+                const float* f = base + (size_t)step * 4 * NE_STRIDE;
+                double frag[6];
 #pragma unroll
-            for (int b = 0; b < 6; b++)
-                frag[b] = (double)f[8 * b];
+                for (int b = 0; b < 6; b++)
+                    frag[b] = (double)f[8 * b];
 #pragma unroll
-            for (int t = 0; t < NE_TILES; t++)
-                dmma_8x8x4(acc[t][0], acc[t][1], frag[tile_i(t)], frag[tile_j(t)]);
+                for (int t = 0; t < NE_TILES; t++)
+                    dmma_8x8x4(acc[t][0], acc[t][1], frag[tile_i(t)], frag[tile_j(t)]);
+            }
         }
     }
 
@@ -176,17 +140,29 @@ __global__ void __launch_bounds__(NE_THREADS, 4) k_ls_accumulate_mma(Planes P, L
         red[((size_t)warp * NE_TILES + t) * 64 + r * 8 + cidx + 1] = acc[t][1];
     }
     __syncthreads();
-    for (int x = tid; x < NE_TILES * 64; x += NE_THREADS)
+    // entry (a, b) of the compact system sits at slots (z_slot(a), z_slot(b)) of the Gram, a <= b read from the upper
+    // block triangle (slot order follows column order, so z_slot(a) <= z_slot(b))
+    for (int e = tid; e < A.entries; e += NE_THREADS)
     {
-        const int t = x / 64, r = (x % 64) / 8, cc = x % 8;
-        const int a = 8 * tile_i(t) + r, b = 8 * tile_j(t) + cc;
-        int e = -1;
-        if (a <= b && b < mm)
-            e = tri_index(a, b, mm);
-        else if (a < mm && b >= mm && b < mm + nout)
-            e = mm * (mm + 1) / 2 + (b - mm) * mm + a;   // rhs of output b - mm (t sits at column mm + c)
-        if (e < 0)
-            continue;
+        const int tri = mm * (mm + 1) / 2;
+        int a, b;
+        if (e < tri)
+        {
+            a = 0;
+            while (e >= tri_index(a, mm - 1, mm) + 1)
+                a++;
+            b = a + (e - tri_index(a, a, mm));
+        }
+        else
+        {
+            a = (e - tri) % mm;
+            b = mm + (e - tri) / mm;
+        }
+        const int sa = z_slot(a, P.c0, P.c1), sb = z_slot(b, P.c0, P.c1);
+        int t = 0;
+        while (!(tile_i(t) == sa / 8 && tile_j(t) == sb / 8))
+            t++;
+        const int r = sa % 8, cc = sb % 8;
         double sum = 0.0;
         for (int w = 0; w < NE_WARPS; w++)
             sum += red[((size_t)w * NE_TILES + t) * 64 + r * 8 + cc];
@@ -220,21 +196,47 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     Planes P = planes_for(d, 0, [&](int) { return (size_t)0; });
     P.kc = k;
     NB_TRY(block_begin(d));
+    NB_TRY(ensure_site_targets(d, k, 0));
+    LsArgs A{ d->ls_partial, entries, {} };
+    A.tgt.t = d->site_tgt;
+    long long ft = 0;
+    for (int i = 0; i < P.n; i++)
+    {
+        A.tgt.site0[i] = ft;
+        ft += (long long)P.p[i].w0 * P.p[i].h0 * k;
+    }
+    A.tgt.site0[P.n] = ft;
     dim3 grid(LS_GRID, (unsigned)P.n);
     if (d->mixed_gram)
     {
         NB_CUDA(cudaMemsetAsync(d->counters + CNT_STATUS, 0, sizeof(unsigned int), d->stream));
         NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
-        NB_TRY(launch_ls_accumulate_tc(d, P, d->ls_partial, entries, d->stream));
+        NB_TRY(launch_ls_accumulate_tc(d, P, d->ls_partial, entries, A.tgt, d->stream));
         NB_TRY(ktimer_end(d));
     }
     else
     {
         const size_t shared = std::max((size_t)NE_THREADS * NE_STRIDE * sizeof(float),
                                        (size_t)NE_WARPS * NE_TILES * 64 * sizeof(double));
-        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
         NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
-        k_ls_accumulate_mma<<<grid, NE_THREADS, shared, d->stream>>>(P, LsArgs{ d->ls_partial, entries });
+#define NB_NE(NO)                                                                                                     \
+    case NO:                                                                                                          \
+        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma<NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared)); \
+        k_ls_accumulate_mma<NO><<<grid, NE_THREADS, shared, d->stream>>>(P, A);                                       \
+        break;
+        switch (d->nout)
+        {
+            NB_NE(3)
+            NB_NE(6)
+            NB_NE(9)
+            NB_NE(12)
+            NB_NE(15)
+            NB_NE(18)
+        default:
+            set_error(NNTC_B200_ERR_STATE, "a material holds 1..6 RGB textures");
+            return NNTC_B200_ERR_STATE;
+        }
+#undef NB_NE
         NB_TRY(ktimer_end(d));
         NB_LAUNCHED();
     }

@@ -67,7 +67,8 @@ constexpr double JOINT_PSNR_SLACK = 0.01;   // dB a texture's base-level PSNR ma
 // along their preconditioned objective gradients by the best of alpha in {1, 1/2, 1/4} (snapped onto their grids, the
 // decoder held), the decoder is re-solved at the step taken, the step is re-packed into BC blocks and refined, and the
 // whole pass is kept only when the shipped E falls below e_ship AND no texture's 8-bit PSNR at the base level falls
-// by more than JOINT_PSNR_SLACK dB; otherwise every part of the state is restored exactly. The guard exists because E
+// by more than JOINT_PSNR_SLACK dB (checked first on the step before the re-pack, which then refuses it without the
+// pack and the refinement); otherwise every part of the state is restored exactly. The guard exists because E
 // is one sum over every texture: a step that lowers it can move error from the textures with the most of it onto
 // the nearly exact ones (a binary metalness map loses decibels to a handful of texels that cross an 8-bit rounding
 // boundary while E barely moves).
@@ -80,6 +81,17 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
     NB_CUDA(cudaEventCreate(&j0));
     NB_CUDA(cudaEventCreate(&j1));
     NB_CUDA(cudaEventRecord(j0, d->stream));
+    // the pass's span, recorded on every way out
+    auto finish = [&](int status) -> int {
+        NB_CUDA(cudaEventRecord(j1, d->stream));
+        NB_CUDA(cudaEventSynchronize(j1));
+        float jm = 0.0f;
+        NB_CUDA(cudaEventElapsedTime(&jm, j0, j1));
+        r->ms_joint = jm;
+        cudaEventDestroy(j0);
+        cudaEventDestroy(j1);
+        return status;
+    };
     r->e_before_joint = e_ship;
     double psnr_before[6] = {};
     NB_TRY(nb::psnr_base(d, m, psnr_before));
@@ -120,6 +132,19 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
         NB_TRY(nb::joint_apply(d, m, k, 0, best));
         NB_TRY(nb::joint_apply(d, m, k, 1, best));
         NB_TRY(block_a());
+        // the guard first on the step itself (its latents on their grids, before the BC re-pack, which only loses
+        // quality): a texture already below the guard here is refused without the pack and the refinement
+        double psnr_step[6] = {};
+        NB_TRY(nb::psnr_base(d, m, psnr_step));
+        bool early = true;
+        for (int t = 0; t < m->textures && t < 6; t++)
+            early = early && psnr_step[t] >= psnr_before[t] - JOINT_PSNR_SLACK;
+        if (!early)
+        {
+            r->joint_taken = -1;
+            NB_TRY(restore());
+            return finish(NNTC_B200_OK);
+        }
         double ms = 0.0;
         NB_TRY(nntc_b200_bc_pack_prepare(d, m, k, 1, nullptr, &ms));
         r->ms_pack += ms;
@@ -144,14 +169,7 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
             st = restore();
         }
     }
-    NB_CUDA(cudaEventRecord(j1, d->stream));
-    NB_CUDA(cudaEventSynchronize(j1));
-    float jm = 0.0f;
-    NB_CUDA(cudaEventElapsedTime(&jm, j0, j1));
-    r->ms_joint = jm;
-    cudaEventDestroy(j0);
-    cudaEventDestroy(j1);
-    return st;
+    return finish(st);
 }
 
 }   // namespace

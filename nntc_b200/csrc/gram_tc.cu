@@ -2,54 +2,83 @@
 // FP32 accumulators in tensor memory, FP64 across batches: the mixed-precision form of the accumulation that
 // decoder.cu's k_ls_accumulate_mma does in FP64 (the sums of src/solve_decoder.cu:87-161).
 //
-// Every entry the decoder's system needs is an entry of the Gram Z^T Z of the site rows Z = [phi | 1 | t] (at most 43
-// columns, padded to 48). A float x is split x = hi + lo with hi = bf16(x) and lo = bf16(x - hi) (x - hi is exact in
-// float), which holds x to about 2^-17 of itself. One CTA stages 128 sites' rows; the rows [Z_hi ; Z_lo] become one
-// K-major operand tile of 128 rows (48 hi, 48 lo, 32 zero) by 16 sites per MMA step, and one MMA of M = 128, N = 96,
-// K = 16 with that tile as both A and B produces the four products of the split at once:
+// Every entry the decoder's system needs is an entry of the Gram Z^T Z of the site rows Z = [phi | 1 | t] (site_z()'s
+// fixed 48-slot layout). A float x is split x = hi + lo with hi = bf16(x) and lo = bf16(x - hi) (x - hi is exact in
+// float), which holds x to about 2^-17 of itself. A stage is 128 sites (site j of the 128 texels of a chunk, one per
+// thread); their rows [Z_hi ; Z_lo] form one operand of 96 rows (48 hi, 48 lo) by 128 sites, and eight MMAs of
+// M = 128, N = 96, K = 16 with that operand as both A and B produce the four products of the split at once:
 //
-//   D = [Z_hi ; Z_lo ; 0] [Z_hi ; Z_lo]^T  =  [[hi hi, hi lo], [lo hi, lo lo], 0]     (128 x 96, FP32, in TMEM)
+//   D = [Z_hi ; Z_lo ; *] [Z_hi ; Z_lo]^T  =  [[hi hi, hi lo], [lo hi, lo lo], *]     (128 x 96, FP32, in TMEM)
 //
 // so Z^T Z = hi hi + hi lo + lo hi + lo lo: the compensated three-product form plus the lo lo term, which costs
-// nothing more here. After every batch of 256 sites the accumulator is read back (row r of D is TMEM lane r) and
-// added into FP64 registers, the hi and lo halves of each column in a fixed order; a CTA writes one partial per
-// entry, which k_ls_reduce folds in block order as it does for the FP64 form. Deterministic: the tensor core's sums of
-// a batch are a fixed function of the tile, the rest is fixed-order FP64.
+// nothing more here. The rows are shifted before the split, z' = z - mu with mu the mean of the CTA's first 128
+// centre sites (the constant's slot not shifted), and the shift is undone on the sums in FP64 at the end: the FP32
+// accumulators then hold sums of small centred products instead of the large mean-dominated ones, whose rounding the
+// decoder's system (nearly collinear with its constant column) would amplify (unshifted, the decoder of a converged
+// state differed from the FP64 form's by 2.4e-4 of its largest coefficient). (A's rows 96..127 are whatever follows in shared memory; the rows of D they produce are never
+// read.) After every batch of 256 sites the rows of D the system reads (phi and 1: 25 hi rows, 25 lo rows; row r of D
+// is TMEM lane r) are read back, the hi and lo halves of each column added in FP32 and the sums added into FP64 rows in
+// shared memory; a CTA writes one partial per entry, which k_ls_reduce folds in block order as it does for the FP64
+// form. Deterministic: the tensor core's sums of a batch are a fixed function of the operand, the rest is fixed-order.
+//
+// The operand is stored MN-major (no swizzle): a core matrix is 8 sites x 8 consecutive rows (16 bytes per site), so
+// each thread writes its site's 96 values as twelve 16-byte stores straight from registers, rows 8g..8g+7 at
+// g x TG_MN, the next eight sites at TG_KG. In the descriptor of this layout (MN-major, no swizzle) the leading byte
+// offset is the K direction's stride and the stride byte offset the MN direction's. The offsets are chosen so that
+// every byte the MMAs can address under either reading of the two strides lies inside the CTA's shared memory
+// (checked at compile time below).
 //
 // The tensor-core plumbing, all by inline PTX: tcgen05.alloc / dealloc of 128 TMEM columns per CTA (three CTAs per SM
-// by registers and shared memory, 384 of the 512 columns, so an allocation never waits on another CTA), shared-memory matrix descriptors of the
-// no-swizzle K-major canonical layout (8-row x 16-byte core matrices, LBO = the K-neighbour's offset, SBO = the next
-// eight rows'), tcgen05.mma.cta_group::1.kind::f16 issued by one thread, tcgen05.commit to an mbarrier, tcgen05.ld of
-// 32 lanes x 32 columns per warp. No TMA, no multicast, no cluster: the operands are built in shared memory by the
-// threads from the planes (the rows are computed, not copied). Every wait on the mbarrier is bounded; a wait that
-// gives up raises the device status word, waits (bounded) once more, frees the tensor memory and leaves.
+// by shared memory, 384 of the 512 columns, so an allocation never waits on another CTA), shared-memory matrix
+// descriptors, tcgen05.mma.cta_group::1.kind::f16 issued by one thread, tcgen05.commit to an mbarrier per operand
+// buffer (two buffers: one stage's MMAs run while the next stage's rows are formed), tcgen05.ld of 32 lanes x 32
+// columns per warp. No TMA, no multicast, no cluster: the operands are computed by the threads, not copied. Every wait
+// on an mbarrier is bounded; a wait that gives up raises the device status word, waits (bounded) once more, frees the
+// tensor memory and leaves.
 
 #include <cstdint>
 
 #include <cuda_bf16.h>
 
 #include "device.cuh"
+#include "site_rows.cuh"
 
 namespace nb
 {
 
-constexpr int TG_THREADS = 128;           // four warps: one TMEM lane quadrant each
-constexpr int TG_SITES = 128;             // sites per stage (one per thread)
-constexpr int TG_KSTEPS = TG_SITES / 16;  // MMAs per stage
-constexpr int TG_STAGES_PER_BATCH = 2;    // FP32 accumulation spans 256 sites
-constexpr int TG_ROW = 57;                // floats per staged site row (odd: conflict-free column reads)
-constexpr int TG_TILE_BYTES = 128 * 16 * 2;   // one K-step operand tile: 128 rows x 16 bf16
-constexpr int TG_TMEM_COLS = 128;         // allocation (power of two >= 96)
-constexpr int TG_BUFFERS = 1;             // operand buffers: one stage's MMAs run while the next stage's site rows
-                                          // are formed; a second buffer (the tile build overlapping too) measured no
-                                          // faster and costs the third CTA per SM
+constexpr int TG_THREADS = 128;                    // four warps; a thread's texel, and TMEM lane = row of D
+constexpr int TG_SITES = 128;                      // sites per stage
+constexpr int TG_KSTEPS = TG_SITES / 16;           // MMAs per stage
+constexpr int TG_BUFFERS = 2;                      // operand buffers
+constexpr int TG_STAGES_PER_BATCH = 2;             // FP32 accumulation spans 256 sites (512 measured
+                                                   // 5x the decoder error at a converged state)
+constexpr uint32_t TG_CORE = 128;                  // one core matrix: 8 sites x 8 rows of bf16
+constexpr uint32_t TG_MN = TG_CORE;                // MN direction: the next eight rows
+constexpr uint32_t TG_KG = 12 * TG_CORE;           // K direction: the next eight sites, after the 12 row groups
+constexpr uint32_t TG_STEP = 2 * TG_KG;            // one K-step of 16 sites
+constexpr uint32_t TG_BUF = TG_KSTEPS * TG_STEP;   // one stage's operand, 24 KB
+constexpr int TG_ROWS = 25;                        // Gram rows the system reads (site_z slots 0..24)
+constexpr int TG_ACC_STRIDE = 49;                  // doubles per FP64 row in shared memory
+constexpr uint32_t TG_ACC_OFFSET = TG_BUFFERS * TG_BUF + 4 * TG_CORE;   // past A's rows 96..127 of the last step
+constexpr uint32_t TG_ACC_BYTES = 2 * TG_ROWS * TG_ACC_STRIDE * sizeof(double);
+constexpr int TG_TMEM_COLS = 128;                  // allocation (power of two >= 96)
 constexpr uint32_t TG_WAIT_LIMIT = 1u << 26;
+
+// The farthest byte an MMA of the last step of the last buffer can address, under either reading of LBO and SBO
+// (16 row groups of A at the larger stride, the second K group at the larger stride, a 16-byte row): the dynamic
+// shared memory is at least this long.
+constexpr uint32_t TG_MAX_STRIDE = TG_MN > TG_KG ? TG_MN : TG_KG;
+constexpr uint32_t TG_REACH = (TG_BUFFERS - 1) * TG_BUF + (TG_KSTEPS - 1) * TG_STEP + 16 * TG_MAX_STRIDE + 16;
+constexpr uint32_t TG_SHARED = TG_ACC_OFFSET + TG_ACC_BYTES > TG_REACH ? TG_ACC_OFFSET + TG_ACC_BYTES : TG_REACH;
+static_assert(TG_SHARED <= 76 * 1024, "three CTAs per SM");
+static_assert(TG_ACC_OFFSET % 16 == 0 && TG_BUF % 16 == 0, "16-byte aligned operand and accumulator regions");
 
 struct TcArgs
 {
     double* partial;        // [plane][entry][LS_GRID]
     int entries;
     unsigned int* status;   // raised on a wait that gave up
+    SiteTargetView tgt;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -68,11 +97,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
     return d;
 }
 
-// The instruction descriptor of kind::f16: FP32 accumulator (bit 4), A and B BF16 (bits 7 and 10), both K-major,
-// N >> 3 at bit 17, M >> 4 at bit 24.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n)
+// The instruction descriptor of kind::f16: FP32 accumulator (bit 4), A and B BF16 (bits 7 and 10), A and B both
+// MN-major (bits 15 and 16), N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int m, int n)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
 }
 
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
@@ -92,78 +122,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
-// Staged site row of Z (phi | 1 | t | zeros) for site `si` of plane V, with the arithmetic of the FP64 form.
-__device__ __forceinline__ void site_row(const Planes& P, const PlaneView& V, size_t si, size_t sites, float* row)
-{
-    const int c0 = P.c0, c1 = P.c1, nout = P.nout, kc = P.kc, per_pixel = 1 + kc;
-    int q = 0;
-    if (si < sites)
-    {
-        const size_t pixel = si / (size_t)per_pixel;
-        const int j = (int)(si % (size_t)per_pixel);
-        const int px = (int)(pixel % (size_t)V.w0), py = (int)(pixel / (size_t)V.w0);
-        float dx, dy;
-        site_offset(kc, j, px, py, dx, dy);
-        float s[MAX_CH], c[MAX_CH], w4[4];
-        blend_u<MAX_CH>(V.v1, V.w1, c1, tap_at(px, py, dx, dy, V.w0, V.h0, V.w1, V.h1), c);
-        Tap t0{};
-        if (j == 0)
-        {
-#pragma unroll
-            for (int i = 0; i < MAX_CH; i++)
-                if (i < c0)
-                    s[i] = __ldg(V.v0 + pixel * c0 + i);
-        }
-        else
-        {
-            t0 = tap_at(px, py, dx, dy, V.w0, V.h0, V.w0, V.h0);
-            blend_u<MAX_CH>(V.v0, V.w0, c0, t0, s);
-            tap_weights(t0, w4);
-        }
-#pragma unroll
-        for (int b = 0; b < MAX_CH; b++)
-            if (b < c1)
-                row[q++] = c[b];
-#pragma unroll
-        for (int i = 0; i < MAX_CH; i++)
-            if (i < c0)
-                row[q++] = s[i];
-#pragma unroll
-        for (int i = 0; i < MAX_CH; i++)
-#pragma unroll
-            for (int b = 0; b < MAX_CH; b++)
-                if (i < c0 && b < c1)
-                    row[q++] = s[i] * c[b];
-        row[q++] = 1.0f;
-        for (int r = 0; r < nout; r++)
-        {
-            float t;
-            if (j == 0)
-                t = __ldg(V.src + pixel * nout + r);
-            else
-                t = w4[0] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x0) * nout + r) +
-                    w4[1] * __ldg(V.src + ((size_t)t0.y0 * V.w0 + t0.x1) * nout + r) +
-                    w4[2] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x0) * nout + r) +
-                    w4[3] * __ldg(V.src + ((size_t)t0.y1 * V.w0 + t0.x1) * nout + r);
-            row[q++] = t;
-        }
-    }
-    for (; q < 48; q++)
-        row[q] = 0.0f;
-}
-
-// Byte offset of (row r, site k) of K-step tile `step` in the canonical no-swizzle K-major layout: core matrix
-// (r / 8, k / 8) of 128 bytes, K-neighbours 128 bytes apart (LBO), row groups 256 bytes apart (SBO).
-__host__ __device__ constexpr uint32_t tile_offset(int step, int r, int k)
-{
-    return (uint32_t)step * TG_TILE_BYTES + (uint32_t)(((r >> 3) * 2 + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
-}
-
-__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 a, __nv_bfloat16 b)
-{
-    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
-}
-
 // 32 columns of this warp's TMEM lane quadrant into registers.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v)
 {
@@ -177,35 +135,67 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v)
                  : "r"(taddr));
 }
 
-__global__ void __launch_bounds__(TG_THREADS, 3) k_ls_accumulate_tc(Planes P, TcArgs A)
+// The batch's FP32 sums into the FP64 rows: warp w holds TMEM lanes 32w..32w+31; row r < 25 (hi) goes to FP64 row r,
+// row 48 + r (lo) to FP64 row 25 + r; columns j (hi) and 48 + j (lo) of D are added first.
+__device__ __forceinline__ void tc_readback(uint32_t tmem, int warp, int lane, double* acc)
 {
-    extern __shared__ __align__(128) unsigned char tg_sh[];
-    // the operand buffers (TG_BUFFERS x TG_KSTEPS tiles of 4 KB), then the staged site rows [site][TG_ROW]
+    if (warp >= 3)
+        return;
+    const int r = warp * 32 + lane;
+    const int row = r < TG_ROWS ? r : (r >= 48 && r < 48 + TG_ROWS ? TG_ROWS + r - 48 : -1);
+    const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
+    float g[48];
+    uint32_t v[32];
+    tmem_ld32(base + 0, v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+        g[j] = __uint_as_float(v[j]);
+    tmem_ld32(base + 32, v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+        g[32 + j] = __uint_as_float(v[j]);
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+        g[j] += __uint_as_float(v[16 + j]);
+    tmem_ld32(base + 64, v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+        g[16 + j] += __uint_as_float(v[j]);
+    if (row >= 0)
+    {
+        double* a = acc + row * TG_ACC_STRIDE;
+#pragma unroll
+        for (int j = 0; j < 48; j++)
+            a[j] += (double)g[j];
+    }
+}
+
+template <int NOUT>
+__global__ void __launch_bounds__(TG_THREADS, 3) k_ls_accumulate_tc(Planes P, const __grid_constant__ TcArgs A)
+{
+    extern __shared__ __align__(1024) unsigned char tg_sh[];
     unsigned char* tiles = tg_sh;
-    float* rows = reinterpret_cast<float*>(tg_sh + TG_BUFFERS * TG_KSTEPS * TG_TILE_BYTES);
-    __shared__ uint64_t mbar[2];
+    double* acc = reinterpret_cast<double*>(tg_sh + TG_ACC_OFFSET);
+    __shared__ uint64_t mbar[TG_BUFFERS];
     __shared__ uint32_t tmem_base;
-    __shared__ int failed;
+    __shared__ __align__(16) float mu[ZS_WIDTH];   // the CTA's shift (zero in the constant's slot)
 
     const int pl = blockIdx.y;
     const PlaneView& V = P.p[pl];
-    const int mm = P.nin + 1, nout = P.nout, kc = P.kc;
-    const size_t sites = (size_t)V.w0 * V.h0 * (1 + kc);
-    const size_t chunks = (sites + TG_SITES - 1) / TG_SITES;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int row_id = tid;   // this thread's TMEM lane (row of D)
+    const int mm = P.nin + 1, kc = P.kc;
+    const long long texels = (long long)V.w0 * V.h0;
+    const long long chunks = (texels + TG_THREADS - 1) / TG_THREADS;
+    const float* tgt = A.tgt.t + (size_t)A.tgt.site0[pl] * NOUT;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    double acc[48];
-#pragma unroll
-    for (int j = 0; j < 48; j++)
-        acc[j] = 0.0;
+    for (int i = tid; i < 2 * TG_ROWS * TG_ACC_STRIDE; i += TG_THREADS)
+        acc[i] = 0.0;
 
-    const bool work = (size_t)blockIdx.x < chunks;
-    if (work)
+    if ((long long)blockIdx.x < chunks)
     {
-        // the zero rows 96..127 of every tile, once; the other rows are rewritten every stage
-        for (int i = tid; i < TG_BUFFERS * TG_KSTEPS * TG_TILE_BYTES / 16; i += TG_THREADS)
-            reinterpret_cast<uint4*>(tiles)[i] = make_uint4(0u, 0u, 0u, 0u);
         if (warp == 0)
         {
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -216,130 +206,172 @@ __global__ void __launch_bounds__(TG_THREADS, 3) k_ls_accumulate_tc(Planes P, Tc
         }
         if (tid == 0)
         {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[0])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[1])) : "memory");
+            for (int x = 0; x < TG_BUFFERS; x++)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[x])) : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            failed = 0;
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tmem = tmem_base;
         const uint32_t tiles_addr = smem_addr(tiles);
-        constexpr uint32_t idesc = umma_idesc_bf16(128, 96);
+        constexpr uint32_t idesc = umma_idesc_bf16_mn(128, 96);
         // per buffer: the parity of its next completion, and whether a commit on it is still unwaited (every thread
-        // keeps the same copy: all take the same branches)
-        uint32_t ph[2] = { 0u, 0u };
-        bool pending[2] = { false, false };
+        // keeps the same copy: all take the same branches); gave_up: one of this thread's waits ran out, which the
+        // next barrier (__syncthreads_or) makes every thread's decision at once
+        // (bit x of each mask for buffer x, so that nothing is indexed at run time)
+        uint32_t ph = 0u, pending = 0u;
+        bool gave_up = false;
         auto settle = [&](int x) {
-            if (!pending[x])
+            const uint32_t bit = 1u << x;
+            if (!(pending & bit))
                 return;
-            if (!mbar_wait(&mbar[x], ph[x]))
-                failed = 1;
-            ph[x] ^= 1u;
-            pending[x] = false;
+            if (!mbar_wait(&mbar[x], (ph >> x) & 1u))
+                gave_up = true;
+            ph ^= bit;
+            pending &= ~bit;
         };
-        int in_batch = 0, stage = 0;
-
-        for (size_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x, stage++)
+        // the shift: the mean of the centre sites of the CTA's first chunk, in a fixed order (rows staged in the first
+        // operand buffer as floats, then one column per thread)
         {
-            const int bsel = stage % TG_BUFFERS;
-            unsigned char* tb = tiles + (size_t)bsel * TG_KSTEPS * TG_TILE_BYTES;
-            // 1. this thread's site row, in float (the MMAs of the previous stage run meanwhile)
-            site_row(P, V, chunk * TG_SITES + tid, sites, rows + tid * TG_ROW);
-            // 2. the buffer's previous MMAs are done before it is overwritten
-            settle(bsel);
-            __syncthreads();
-            if (failed)
-                break;
-            // 3. the operand tiles: item (column f, 8-site group g) packs 8 sites of column f into 16 bytes, hi into
-            //    row f and lo into row 48 + f
-            for (int it = tid; it < 48 * (TG_SITES / 8); it += TG_THREADS)
-            {
-                const int f = it % 48, g = it / 48;
-                uint32_t hi[4], lo[4];
+            const long long pixel = (long long)blockIdx.x * TG_THREADS + tid;
+            const bool valid = pixel < texels;
+            float z[ZS_WIDTH];
+            if (valid)
+                site_z<NOUT>(P, V, tgt, pixel, (int)(pixel % V.w0), (int)(pixel / V.w0), 0, z);
+            float* rows = reinterpret_cast<float*>(tiles);   // [TG_THREADS][ZS_WIDTH + 1]
 #pragma unroll
-                for (int q = 0; q < 8; q += 2)
-                {
-                    const float x0 = rows[(g * 8 + q) * TG_ROW + f], x1 = rows[(g * 8 + q + 1) * TG_ROW + f];
-                    const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-                    const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-                    const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-                    hi[q / 2] = pack_bf16x2(h0, h1);
-                    lo[q / 2] = pack_bf16x2(l0, l1);
-                }
-                const int step = g / 2, k = (g & 1) * 8;
-                *reinterpret_cast<uint4*>(tb + tile_offset(step, f, k)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                *reinterpret_cast<uint4*>(tb + tile_offset(step, 48 + f, k)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-            }
-            // generic-proxy stores become visible to the tensor core's async proxy; the rows are free again
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            for (int q = 0; q < ZS_WIDTH; q++)
+                rows[tid * (ZS_WIDTH + 1) + q] = valid ? z[q] : 0.0f;
             __syncthreads();
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // 4. one thread issues the stage's MMAs and commits them to the buffer's barrier; nobody waits here
-            if (tid == 0)
+            if (tid < ZS_WIDTH)
             {
-                const uint32_t base = tiles_addr + (uint32_t)bsel * TG_KSTEPS * TG_TILE_BYTES;
-                for (int s = 0; s < TG_KSTEPS; s++)
+                const int n = (int)min((long long)TG_THREADS, texels - (long long)blockIdx.x * TG_THREADS);
+                float sum = 0.0f;
+                for (int t = 0; t < n; t++)
+                    sum += rows[t * (ZS_WIDTH + 1) + tid];
+                mu[tid] = tid == ZS_ONE ? 0.0f : sum / (float)n;
+            }
+            __syncthreads();
+        }
+        // this thread's site within a stage: K-step tid / 16, K group (tid / 8) % 2, row tid % 8 of its core matrices
+        const uint32_t my_site = (uint32_t)(tid >> 4) * TG_STEP + (uint32_t)((tid >> 3) & 1) * TG_KG +
+                                 (uint32_t)(tid & 7) * 16;
+        int in_batch = 0, stage = 0;
+        bool stop = false;
+
+        for (long long chunk = blockIdx.x; chunk < chunks && !stop; chunk += gridDim.x)
+        {
+            const long long pixel = chunk * TG_THREADS + tid;
+            const bool valid = pixel < texels;
+            const int px = valid ? (int)(pixel % V.w0) : 0, py = valid ? (int)(pixel / V.w0) : 0;
+            for (int j = 0; j <= kc; j++, stage++)
+            {
+                const int bsel = stage % TG_BUFFERS;
+                // 1. this thread's site row, split hi + lo in registers (the previous stage's MMAs run meanwhile)
+                float z[ZS_WIDTH];
+                if (valid)
                 {
-                    const uint64_t desc = umma_desc(base + (uint32_t)s * TG_TILE_BYTES, 128, 256);
-                    const uint32_t accumulate = (in_batch > 0 || s > 0) ? 1u : 0u;
-                    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                                 "l"(desc), "l"(desc), "r"(idesc), "r"(accumulate)
+                    site_z<NOUT>(P, V, tgt, pixel, px, py, j, z);
+#pragma unroll
+                    for (int q = 0; q < ZS_WIDTH; q += 4)
+                    {
+                        const float4 m4 = *reinterpret_cast<const float4*>(mu + q);
+                        z[q] -= m4.x;
+                        z[q + 1] -= m4.y;
+                        z[q + 2] -= m4.z;
+                        z[q + 3] -= m4.w;
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int q = 0; q < ZS_WIDTH; q++)
+                        z[q] = 0.0f;
+                }
+                uint32_t hi[ZS_WIDTH / 2], lo[ZS_WIDTH / 2];
+#pragma unroll
+                for (int q = 0; q < ZS_WIDTH / 2; q++)
+                {
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(z[2 * q], z[2 * q + 1]);
+                    const float2 hf = __bfloat1622float2(h);
+                    const __nv_bfloat162 l = __floats2bfloat162_rn(z[2 * q] - hf.x, z[2 * q + 1] - hf.y);
+                    hi[q] = *reinterpret_cast<const uint32_t*>(&h);
+                    lo[q] = *reinterpret_cast<const uint32_t*>(&l);
+                }
+                // 2. the buffer's previous MMAs are done before it is overwritten
+                settle(bsel);
+                unsigned char* at = tiles + (size_t)bsel * TG_BUF + my_site;
+#pragma unroll
+                for (int g = 0; g < 6; g++)
+                {
+                    *reinterpret_cast<uint4*>(at + g * TG_MN) =
+                        make_uint4(hi[4 * g], hi[4 * g + 1], hi[4 * g + 2], hi[4 * g + 3]);
+                    *reinterpret_cast<uint4*>(at + (6 + g) * TG_MN) =
+                        make_uint4(lo[4 * g], lo[4 * g + 1], lo[4 * g + 2], lo[4 * g + 3]);
+                }
+                // generic-proxy stores become visible to the tensor core's async proxy
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (__syncthreads_or(gave_up))
+                {
+                    stop = true;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                // 3. one thread issues the stage's MMAs and commits them to the buffer's barrier; nobody waits here
+                if (tid == 0)
+                {
+                    const uint32_t base = tiles_addr + (uint32_t)bsel * TG_BUF;
+                    for (int s = 0; s < TG_KSTEPS; s++)
+                    {
+                        const uint64_t desc = umma_desc(base + (uint32_t)s * TG_STEP, TG_KG, TG_MN);
+                        const uint32_t accumulate = (in_batch > 0 || s > 0) ? 1u : 0u;
+                        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                                     "l"(desc), "l"(desc), "r"(idesc), "r"(accumulate)
+                                     : "memory");
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_addr(&mbar[bsel]))
                                  : "memory");
                 }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_addr(&mbar[bsel]))
-                             : "memory");
-            }
-            pending[bsel] = true;
-            const bool last = chunk + gridDim.x >= chunks;
-            if (++in_batch == TG_STAGES_PER_BATCH || last)
-            {
-                // 5. the batch's MMAs done, its FP32 sums into FP64: row r of D, columns j (hi) and 48 + j (lo)
-                settle(0);
-                settle(1);
-                __syncthreads();
-                if (failed)
-                    break;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                if (warp < 3)
+                pending |= 1u << bsel;
+                if (++in_batch == TG_STAGES_PER_BATCH)
                 {
-                    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-                    uint32_t v[32];
-                    tmem_ld32(lane_base + 0, v);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int j = 0; j < 32; j++)
-                        acc[j] += (double)__uint_as_float(v[j]);
-                    tmem_ld32(lane_base + 32, v);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        acc[32 + j] += (double)__uint_as_float(v[j]);
-#pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        acc[j] += (double)__uint_as_float(v[16 + j]);
-                    tmem_ld32(lane_base + 64, v);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int j = 0; j < 32; j++)
-                        acc[16 + j] += (double)__uint_as_float(v[j]);
+                    // 4. the batch's MMAs done, its FP32 sums into the FP64 rows
+                    for (int x = 0; x < TG_BUFFERS; x++)
+                        settle(x);
+                    if (__syncthreads_or(gave_up))
+                    {
+                        stop = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    tc_readback(tmem, warp, lane, acc);
+                    in_batch = 0;
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncthreads();
                 }
-                in_batch = 0;
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncthreads();
             }
         }
-        if (failed)
+        if (!stop && in_batch > 0)
+        {
+            for (int x = 0; x < TG_BUFFERS; x++)
+                settle(x);
+            if (!__syncthreads_or(gave_up))
+            {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                tc_readback(tmem, warp, lane, acc);
+            }
+        }
+        if (__syncthreads_or(gave_up))
         {
             if (tid == 0)
                 atomicOr(A.status, 1u);
             // bounded: whatever the tensor core still holds of this CTA's work
-            for (int x = 0; x < 2; x++)
-                if (pending[x])
-                    mbar_wait(&mbar[x], ph[x]);
+            for (int x = 0; x < TG_BUFFERS; x++)
+                if (pending & (1u << x))
+                    mbar_wait(&mbar[x], (ph >> x) & 1u);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
@@ -349,41 +381,65 @@ __global__ void __launch_bounds__(TG_THREADS, 3) k_ls_accumulate_tc(Planes P, Tc
                          : "memory");
     }
 
-    // the hi and lo rows of each Gram row added, then the entries the system needs, one partial per block
+    // entry (a, b) of the compact system from the shifted sums c (FP64 rows z_slot(a) (hi) plus 25 + z_slot(a) (lo),
+    // column z_slot(b)): with z = z' + mu and the constant's slot unshifted, sum z_a z_b = c_ab + mu_a c_1b + mu_b c_1a
+    // + mu_a mu_b c_11, in FP64
     __syncthreads();
-    double* red = reinterpret_cast<double*>(tg_sh);   // [96][49] doubles: every row's sums
-    if (row_id < 96)
+    const bool shifted = (long long)blockIdx.x < chunks;
+    auto cs = [&](int r, int col) {
+        return acc[r * TG_ACC_STRIDE + col] + acc[(TG_ROWS + r) * TG_ACC_STRIDE + col];
+    };
+    const int tri = mm * (mm + 1) / 2;
+    for (int e = tid; e < A.entries; e += TG_THREADS)
     {
-#pragma unroll
-        for (int j = 0; j < 48; j++)
-            red[row_id * 49 + j] = acc[j];
-    }
-    __syncthreads();
-    if (row_id < mm)
-    {
-        const int a = row_id;
-        for (int b = a; b < mm + nout; b++)
+        int a, b;
+        if (e < tri)
         {
-            const double g = red[a * 49 + b] + red[(48 + a) * 49 + b];
-            const int e = b < mm ? tri_index(a, b, mm) : mm * (mm + 1) / 2 + (b - mm) * mm + a;
-            A.partial[((size_t)pl * A.entries + e) * LS_GRID + blockIdx.x] = g;
+            a = 0;
+            while (e >= tri_index(a, mm - 1, mm) + 1)
+                a++;
+            b = a + (e - tri_index(a, a, mm));
         }
+        else
+        {
+            a = (e - tri) % mm;
+            b = mm + (e - tri) / mm;
+        }
+        const int sa = z_slot(a, P.c0, P.c1), sb = z_slot(b, P.c0, P.c1);
+        double g = cs(sa, sb);
+        if (shifted)
+        {
+            const double ma = (double)mu[sa], mb = (double)mu[sb];
+            g += ma * cs(ZS_ONE, sb) + mb * cs(ZS_ONE, sa) + ma * mb * cs(ZS_ONE, ZS_ONE);
+        }
+        A.partial[((size_t)pl * A.entries + e) * LS_GRID + blockIdx.x] = g;
     }
 }
 
-size_t ls_tc_shared_bytes()
+int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries,
+                            const SiteTargetView& tgt, cudaStream_t stream)
 {
-    const size_t stage = (size_t)TG_BUFFERS * TG_KSTEPS * TG_TILE_BYTES + (size_t)TG_SITES * TG_ROW * sizeof(float);
-    const size_t sums = (size_t)96 * 49 * sizeof(double);
-    return stage > sums ? stage : sums;
-}
-
-int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries, cudaStream_t stream)
-{
-    const size_t shared = ls_tc_shared_bytes();
-    NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared));
     dim3 grid(LS_GRID, (unsigned)P.n);
-    k_ls_accumulate_tc<<<grid, TG_THREADS, shared, stream>>>(P, TcArgs{ partial, entries, d->counters + CNT_STATUS });
+    const TcArgs args{ partial, entries, d->counters + CNT_STATUS, tgt };
+#define NB_TC(NO)                                                                                                     \
+    case NO:                                                                                                          \
+        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_tc<NO>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                                     (int)TG_SHARED));                                                                \
+        k_ls_accumulate_tc<NO><<<grid, TG_THREADS, TG_SHARED, stream>>>(P, args);                                     \
+        break;
+    switch (d->nout)
+    {
+        NB_TC(3)
+        NB_TC(6)
+        NB_TC(9)
+        NB_TC(12)
+        NB_TC(15)
+        NB_TC(18)
+    default:
+        set_error(NNTC_B200_ERR_STATE, "a material holds 1..6 RGB textures");
+        return NNTC_B200_ERR_STATE;
+    }
+#undef NB_TC
     NB_LAUNCHED();
     return NNTC_B200_OK;
 }
