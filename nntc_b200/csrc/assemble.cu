@@ -33,6 +33,31 @@ namespace nb
 
 constexpr int SITE_THREADS = 256;
 constexpr int GATHER_THREADS = 128;
+constexpr int GATHER_RING = 6;   // visits in flight per thread on the interior walk (cp.async into shared memory)
+
+// One visit's operands, staged by cp.async: the site's sample of the other latent and (self slot) its gradient term.
+struct __align__(16) VisitSlot
+{
+    float4 y;
+    double t[MAX_CH];
+};
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // The ten products y_i y_k (i <= k < 4) of the monomial layout, row by row: (0,0) (0,1) (0,2) (0,3) (1,1) (1,2)
 // (1,3) (2,2) (2,3) (3,3). Functions rather than tables, so an unrolled index folds to a register name.
@@ -426,16 +451,9 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
     // same floats) and its monomials in a fixed layout: the constant, the four linear terms, then the ten products
     // (i <= k) row by row; a narrower latent uses the entries whose indices are all below its channel count, which is
     // the reference's order
-    auto visit_y = [&](size_t site, float4 y4, float w_self, float w_other) {
+    // the sums' part of a visit (every slot)
+    auto visit_sums = [&](float4 y4, float w_self, float w_other) {
         const float y[MAX_CH] = { y4.x, y4.y, y4.z, y4.w };
-        if (slot == 0)
-        {
-            const double* ts = terms + site * c;
-#pragma unroll
-            for (int a = 0; a < MAX_CH; a++)
-                if (a < c)
-                    g[a] += (double)w_self * ts[a];
-        }
         const TS scale = (TS)w_self * (TS)w_other;
         sums[0] += scale * (TS)1;
 #pragma unroll
@@ -450,6 +468,17 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
                 sums[5 + p] += scale * ((TS)y[i] * (TS)y[k2]);
         }
     };
+    auto visit_y = [&](size_t site, float4 y4, float w_self, float w_other) {
+        if (slot == 0)
+        {
+            const double* ts = terms + site * c;
+#pragma unroll
+            for (int a = 0; a < MAX_CH; a++)
+                if (a < c)
+                    g[a] += (double)w_self * ts[a];
+        }
+        visit_sums(y4, w_self, w_other);
+    };
     auto visit = [&](int px, int py, int j, float w_self, float w_other) {
         const size_t site = (size_t)(py * V.w0 + px) * per + j;
         visit_y(site, __ldg(ys + site), w_self, w_other);
@@ -462,31 +491,96 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
         const int cls = LEVEL0 ? (tx & 1) + 2 * (ty & 1) : 0;
         const int bx = LEVEL0 ? tx : 4 * tx, by = LEVEL0 ? ty : 4 * ty;
         const int e0 = A.gt.off[cls][slot], e1 = A.gt.off[cls][slot + 1];
-        // one visit ahead: the next entry and its sample are loaded while this one is added (the sums still take the
-        // visits in table order)
         auto site_of = [&](const int4& en) {
             return (size_t)((by + ((en.x >> 8) & 0xff) - 64) * V.w0 + (bx + (en.x & 0xff) - 64)) * per + (en.x >> 16);
         };
-        if (e0 < e1)
+        if constexpr (LEVEL0)
         {
-            int4 en = __ldg(A.tab + e0);
-            size_t site = site_of(en);
-            float4 y4 = __ldg(ys + site);
-            for (int e = e0; e < e1; e++)
+            // a level-0 texel meets a dozen or so sites per slot: one visit ahead (the next entry and its sample are
+            // loaded while this one is added), at the occupancy of a kernel without the ring's shared memory
+            if (e0 < e1)
             {
-                int4 nen = en;
-                size_t nsite = site;
-                float4 ny4 = y4;
-                if (e + 1 < e1)
+                int4 en = __ldg(A.tab + e0);
+                size_t site = site_of(en);
+                float4 y4 = __ldg(ys + site);
+                for (int e = e0; e < e1; e++)
                 {
-                    nen = __ldg(A.tab + e + 1);
-                    nsite = site_of(nen);
-                    ny4 = __ldg(ys + nsite);
+                    int4 nen = en;
+                    size_t nsite = site;
+                    float4 ny4 = y4;
+                    if (e + 1 < e1)
+                    {
+                        nen = __ldg(A.tab + e + 1);
+                        nsite = site_of(nen);
+                        ny4 = __ldg(ys + nsite);
+                    }
+                    visit_y(site, y4, __int_as_float(en.y), __int_as_float(en.z));
+                    en = nen;
+                    site = nsite;
+                    y4 = ny4;
                 }
-                visit_y(site, y4, __int_as_float(en.y), __int_as_float(en.z));
-                en = nen;
-                site = nsite;
-                y4 = ny4;
+            }
+        }
+        else
+        {
+            // Level 1's walk (a few hundred visits per texel) keeps GATHER_RING visits in flight: visit e's sample
+            // (and gradient term) is copied into this thread's ring slot e % GATHER_RING by cp.async GATHER_RING
+            // visits before it is added, so that many L2 reads per thread overlap without holding registers; the
+            // sums still take the visits in table order. A slot is refilled only after its visit's values are used.
+            __shared__ VisitSlot ring[GATHER_RING][GATHER_THREADS];
+            float wsq[GATHER_RING], woq[GATHER_RING];
+            const bool grad = slot == 0;
+            auto issue = [&](int i, int e) {
+                const int4 en = __ldg(A.tab + e);
+                wsq[i] = __int_as_float(en.y);
+                woq[i] = __int_as_float(en.z);
+                const size_t site = site_of(en);
+                VisitSlot& rs = ring[i][threadIdx.x];
+                cp_async16(&rs.y, ys + site);
+                if (grad)
+                {
+                    if (c == MAX_CH)
+                    {
+                        cp_async16(&rs.t[0], terms + site * MAX_CH);
+                        cp_async16(&rs.t[2], terms + site * MAX_CH + 2);
+                    }
+                    else
+                    {
+                        for (int a = 0; a < c; a++)
+                            rs.t[a] = __ldg(terms + site * c + a);
+                    }
+                }
+            };
+    #pragma unroll
+            for (int i = 0; i < GATHER_RING; i++)
+            {
+                if (e0 + i < e1)
+                    issue(i, e0 + i);
+                cp_async_commit();
+            }
+            for (int e = e0; e < e1; e += GATHER_RING)
+            {
+    #pragma unroll
+                for (int i = 0; i < GATHER_RING; i++)
+                {
+                    if (e + i < e1)
+                    {
+                        // every group but the newest GATHER_RING - 1 has landed: visit e + i's among them
+                        cp_async_wait<GATHER_RING - 1>();
+                        const VisitSlot& rs = ring[i][threadIdx.x];
+                        if (grad)
+                        {
+    #pragma unroll
+                            for (int a = 0; a < MAX_CH; a++)
+                                if (a < c)
+                                    g[a] += (double)wsq[i] * rs.t[a];
+                        }
+                        visit_sums(rs.y, wsq[i], woq[i]);
+                        if (e + i + GATHER_RING < e1)
+                            issue(i, e + i + GATHER_RING);
+                    }
+                    cp_async_commit();
+                }
             }
         }
     }
@@ -516,7 +610,7 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
 
     // the slot's block, expanded once against the monomial matrices in the reference's order (src/solve_level1.cu:382-399);
     // level 1 expands it in two halves of eight entries (each entry's own sum still in monomial order) so that fewer
-    // doubles are live at once and seven blocks fit an SM
+    // doubles are live at once and six blocks (as many as the visit rings' shared memory allows) fit an SM
     // (where the gradient's store goes changes only which registers are live when: each level's place is the one that
     // spills least at its occupancy)
     auto store_grad = [&]() {
@@ -569,7 +663,7 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather_level0(Planes P, cons
 }
 
 template <typename TS>
-__global__ void __launch_bounds__(GATHER_THREADS, 7) k_gather_level1(Planes P, const __grid_constant__ GatherArgs A)
+__global__ void __launch_bounds__(GATHER_THREADS, 6) k_gather_level1(Planes P, const __grid_constant__ GatherArgs A)
 {
     gather_body<false, TS>(P, A);
 }

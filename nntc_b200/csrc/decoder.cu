@@ -221,7 +221,8 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
         NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
 #define NB_NE(NO)                                                                                                     \
     case NO:                                                                                                          \
-        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma<NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shared)); \
+        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_mma<NO>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                     (int)shared));                                                                   \
         k_ls_accumulate_mma<NO><<<grid, NE_THREADS, shared, d->stream>>>(P, A);                                       \
         break;
         switch (d->nout)

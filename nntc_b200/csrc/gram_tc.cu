@@ -15,11 +15,12 @@
 // centre sites (the constant's slot not shifted), and the shift is undone on the sums in FP64 at the end: the FP32
 // accumulators then hold sums of small centred products instead of the large mean-dominated ones, whose rounding the
 // decoder's system (nearly collinear with its constant column) would amplify (unshifted, the decoder of a converged
-// state differed from the FP64 form's by 2.4e-4 of its largest coefficient). (A's rows 96..127 are whatever follows in shared memory; the rows of D they produce are never
-// read.) After every batch of 256 sites the rows of D the system reads (phi and 1: 25 hi rows, 25 lo rows; row r of D
-// is TMEM lane r) are read back, the hi and lo halves of each column added in FP32 and the sums added into FP64 rows in
-// shared memory; a CTA writes one partial per entry, which k_ls_reduce folds in block order as it does for the FP64
-// form. Deterministic: the tensor core's sums of a batch are a fixed function of the operand, the rest is fixed-order.
+// state differed from the FP64 form's by 2.4e-4 of its largest coefficient). A's rows 96..127 are whatever follows
+// in shared memory; the rows of D they produce are never read. After every batch of 256 sites the rows of D the
+// system reads (phi and 1: 25 hi rows, 25 lo rows; row r of D is TMEM lane r) are read back, the hi and lo halves of
+// each column added in FP32 and the sums added into FP64 rows in shared memory; a CTA writes one partial per entry,
+// which k_ls_reduce folds in block order as it does for the FP64 form. Deterministic: the tensor core's sums of a
+// batch are a fixed function of the operand, the rest is fixed-order.
 //
 // The operand is stored MN-major (no swizzle): a core matrix is 8 sites x 8 consecutive rows (16 bytes per site), so
 // each thread writes its site's 96 values as twelve 16-byte stores straight from registers, rows 8g..8g+7 at
