@@ -355,15 +355,15 @@ def main():
         pipes = {"fp64_tflops": round(fp64.value, 2), "fp32_tflops": round(fp32.value, 2),
                  "how": "nntc_b200_measure_fma_peaks: 8 independent FMA chains per thread, 4 blocks per SM, CUDA events"}
         dom = max(stats, key=lambda k: stats[k][1])
-        roof = roofline(dom, stats[dom], mat, hbm, tf, src)
+        roof = roofline(dom, stats[dom], mat, hbm, tf, src, headline)
         fractions = {}
         for name, st in stats.items():
             if st[0] == 0:
                 continue
             per_launch_s = st[1] / st[0] / 1000.0
             entry = {"ms_per_launch": round(st[1] / st[0], 4),
-                     "hbm_frac": round(algorithmic_bytes(name, mat) / per_launch_s / 1e9 / hbm, 4),
-                     "binding": BINDING.get(name)}
+                     "hbm_frac": round(algorithmic_bytes(name, mat, headline) / per_launch_s / 1e9 / hbm, 4),
+                     "binding": BINDING[headline].get(name)}
             fl = algorithmic_flops(name, mat)
             if fl:
                 pipe = "fp32" if headline == "adjoint" else "fp64"
@@ -467,43 +467,71 @@ def crop_gpu_mpix(L, crop, ea):
     return crop.width * crop.height / 1e6 / (statistics.median(ms) / 1000.0)
 
 
-# DRAM bytes (read + write) per launch of each timed kernel group, per level-0 pixel of the chain, from one ncu capture
-# (--set full) of the 4 x 2048 x 1024 material; a launch's traffic grows with the pixels it covers, so the bench scales
-# these to its own workload. Groups whose kernels changed since their last capture (the assembly's site terms and the
-# objective now read the fractional sites' precomputed targets) have no entry, and their traffic is reported as null.
+# DRAM bytes (read + write) per launch of each timed kernel group, per level-0 pixel of the chain, from ncu captures
+# (one launch of each kernel, its sections and dram__bytes_{read,write}.sum) of the 4 x 2048 x 1024 material (2796160
+# level-0 pixels); a launch's traffic grows with the pixels it covers, so the bench scales these to its own workload.
+# A group of two kernels (the assembly: site terms, then the gather) adds both. Per form: the two forms run different
+# kernels for most groups.
+_PIX3 = 2796160
 TRAFFIC_PER_UNIT = {
-    "normal_equations": 187554048 / 2796160,
-    "bc_refine": 1193938312 / 2796160,                       # one colour
+    "adjoint": {
+        "normal_equations": (723597056 + 8700928) / _PIX3,                    # k_ls_accumulate_tc<12>
+        "objective": (718757888 + 4184064) / _PIX3,                           # k_objective_f32<12>
+        "assemble_level0": (718829056 + 627887616 + 671612160 + 943460608) / _PIX3,
+        "assemble_level1": (718788608 + 627927552 + 885506560 + 71808000) / _PIX3,
+        "quant_sweep": (608629248 + 41608448) / _PIX3,                        # a level-0 colour launch
+        "bc_refine": (1151548000 + 42135040) / _PIX3,                         # one colour
+    },
+    "plain": {
+        "normal_equations": (722979328 + 8198656) / _PIX3,                    # k_ls_accumulate_mma<12>
+        "quant_sweep": (1030932000 + 46642944) / _PIX3,
+        "bc_refine": (1151548000 + 42135040) / _PIX3,
+    },
 }
 
 # What bounds each group, from the same captures: the roofline the HBM fraction alone does not show.
 BINDING = {
-    "assemble_level0": "FP32/ALU issue (site terms) and FP64 issue plus stencil stores (gather); not HBM",
-    "assemble_level1": "FP32/ALU issue (site terms) and L2 latency (gather); not HBM",
-    "objective": "FP64 pipe (~50% of peak)",
-    "normal_equations": "site-row formation (FP32/ALU issue); the tensor pipe (tcgen05, adjoint form) or the FP64 "
-                        "tensor pipe (plain form) is not the bound",
-    "bc_refine": "latency: the set-up's scattered stencil reads, then the ordered selector steps (four evaluated at once)",
-    "quant_sweep": "HBM (level-0 colour launch ~79% of measured copy bandwidth)",
-    "cg_product_level0": "HBM (plain form, FP64 stencil) / FP32 issue (adjoint form, matrix-free)",
-    "cg_product_level1": "HBM (plain form, FP64 stencil) / FP32 issue (adjoint form, matrix-free)",
+    "adjoint": {
+        "assemble_level0": "issue: the fused FP32 site terms at ~88% issue; the gather's L2 latency (one visit ahead)",
+        "assemble_level1": "issue: the fused FP32 site terms at ~88% issue; the gather at ~50% issue (cp.async ring)",
+        "objective": "issue: FP32 decode with fused multiply-adds, ~72% issue, FP32 pipe ~36%",
+        "normal_equations": "latency of the site rows' loads at 12 warps per SM; the tensor pipe (tcgen05) ~14% busy",
+        "bc_refine": "latency: the set-up's scattered stencil reads (~2.3x the needed bytes), then the ordered "
+                     "selector steps",
+        "quant_sweep": "HBM (FP32 stencil, a level-0 colour at ~62% of the copy bandwidth)",
+        "cg_product_level0": "HBM (FP32 stencil)",
+        "cg_product_level1": "DRAM latency (small launches)",
+    },
+    "plain": {
+        "assemble_level0": "FP32/ALU issue (site terms, the reference's unfused arithmetic) and FP64 issue plus stencil "
+                           "stores (gather)",
+        "assemble_level1": "FP32/ALU issue (site terms) and L2 latency (gather)",
+        "objective": "FP64 pipe (~50% of peak)",
+        "normal_equations": "the FP64 tensor pipe (mma.sync m8n8k4, ~76% busy)",
+        "bc_refine": "latency: the set-up's scattered stencil reads (~2.3x the needed bytes), then the ordered "
+                     "selector steps",
+        "quant_sweep": "HBM (FP64 stencil, a level-0 colour at ~78% of the copy bandwidth)",
+        "cg_product_level0": "HBM (FP64 stencil)",
+        "cg_product_level1": "DRAM latency (small launches)",
+    },
 }
 
 
-def roofline(name, stat, mat, hbm, tf, src):
+def roofline(name, stat, mat, hbm, tf, src, form):
     """The dominant kernel against the HBM roofline: its algorithmic bytes per launch over its mean launch time."""
     launches, ms = stat
     if launches == 0:
         return None
-    per = algorithmic_bytes(name, mat)
+    per = algorithmic_bytes(name, mat, form)
     achieved = per / (ms / launches / 1000.0) / 1e9
     t0 = sum(p[0] * p[1] for p in mat.planes)
-    traffic = round(TRAFFIC_PER_UNIT[name] * t0) if name in TRAFFIC_PER_UNIT else None
+    unit = TRAFFIC_PER_UNIT[form].get(name)
+    traffic = round(unit * t0) if unit else None
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_source": src,
             "traffic_source": "ncu DRAM bytes of the 4x2048x1024 workload scaled by level-0 pixels" if traffic
             else "no ncu DRAM figure recorded for this group's current kernels",
-            "binding": BINDING.get(name), "bytes_per_launch": per, "launches": launches,
+            "binding": BINDING[form].get(name), "bytes_per_launch": per, "launches": launches,
             "ms_per_launch": round(ms / launches, 4)}
 
 
@@ -519,24 +547,28 @@ def algorithmic_flops(name, mat):
     return 0
 
 
-def algorithmic_bytes(name, mat):
-    """Bytes a launch must read and write at least (every plane of the chain): its inputs once and its outputs once."""
-    c0, c1, nout = mat.c0, mat.c1, 3 * len(mat.textures)
+def algorithmic_bytes(name, mat, form):
+    """Bytes a launch must read and write at least (every plane of the chain): its inputs once and its outputs once.
+    The stencil is FP64 in the plain form, FP32 in the adjoint form; the targets are the centre sites' source and the
+    fractional sites' cached float targets."""
+    c0, c1, nout, k = mat.c0, mat.c1, 3 * len(mat.textures), mat.k
     t0 = sum(p[0] * p[1] for p in mat.planes)
     t1 = sum(p[2] * p[3] for p in mat.planes)
-    if name == "assemble_level0":   # reads src, v0 (and v1), writes the FP64 stencil and gradient
-        return t0 * (4 * nout + 4 * c0 + 5 * c0 * c0 * 8 + 8 * c0) + t1 * 4 * c1
+    sb = 4 if form == "adjoint" else 8   # bytes per stencil entry
+    targets = 4 * nout * (1 + k)
+    if name == "assemble_level0":   # reads the targets, v0 and v1, writes the stencil and the gradient
+        return t0 * (targets + 4 * c0 + 5 * c0 * c0 * sb + 8 * c0) + t1 * 4 * c1
     if name == "assemble_level1":
-        return t0 * (4 * nout + 4 * c0) + t1 * (4 * c1 + 5 * c1 * c1 * 8 + 8 * c1)
+        return t0 * (targets + 4 * c0) + t1 * (4 * c1 + 5 * c1 * c1 * sb + 8 * c1)
     if name == "objective" or name == "normal_equations":
-        return t0 * (4 * nout + 4 * c0) + t1 * 4 * c1
+        return t0 * (targets + 4 * c0) + t1 * 4 * c1
     if name == "cg_product_level0":   # the stencil's 5 blocks + x in + y out per level-0 texel
-        return t0 * (5 * c0 * c0 * 8 + 3 * 8 * c0)
+        return t0 * (5 * c0 * c0 * sb + 3 * 8 * c0)
     if name == "cg_product_level1":
-        return t1 * (5 * c1 * c1 * 8 + 3 * 8 * c1)
-    if name == "quant_sweep":   # one colour: a quarter of the texels read their 9 blocks' worth
-        return max(t0 * (5 * c0 * c0 * 8 + 2 * 8 * c0 + 9 * c0) // 4 * 4 // 4, t1 * (5 * c1 * c1 * 8) // 4)
-    if name == "bc_refine":   # one colour: a quarter of the blocks read their stencil, grad, planes
+        return t1 * (5 * c1 * c1 * sb + 3 * 8 * c1)
+    if name == "quant_sweep":   # one colour: a quarter of the texels, their 5 own blocks, gradient and state
+        return max(t0 * (5 * c0 * c0 * sb + 2 * 8 * c0 + 9 * c0) // 4, t1 * (5 * c1 * c1 * sb) // 4)
+    if name == "bc_refine":   # one colour: a quarter of the blocks read their FP64 stencil, grad, planes
         return t0 * (5 * c0 * c0 * 8 + 8 * c0 + 4 * c0 + 4 * c0 + 8 * c0) // 4
     return 0
 
