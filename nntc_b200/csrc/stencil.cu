@@ -1170,10 +1170,11 @@ int sweep_block(nntc_b200_device* d, const nntc_b200_model* m, int k, double rid
     const int nc = level0 ? d->c0 : d->c1;
     for (int i = 0; i < np; i++)
         rep[i] = nntc_b200_plane_report{};
-    // the adjoint form: the gradient and the diagonal blocks assembled, the products matrix-free (adjoint_cg.cu)
-    const bool adjoint = d->adjoint_cg != 0 && k <= 4;
+    // every slot assembled whatever the conjugate gradients' operator: a sweep step reads the texel's coupling to its
+    // eight neighbours from the stencil (with the matrix-free option on, an assembly of the diagonal blocks alone
+    // would leave the sweeps reading another block's off-diagonal slots)
     NB_TRY(block_begin(d));
-    NB_TRY(assemble(d, m, k, ridge, level0, adjoint));
+    NB_TRY(assemble(d, m, k, ridge, level0, false));
     NB_CUDA(cudaEventRecord(d->ev[2], d->stream));
     Planes P = texel_planes(d, level0, k);
     k_snapshot<<<(int)(P.start[P.n] / THREADS), THREADS, 0, d->stream>>>(P);

@@ -7,6 +7,8 @@
   texture's base-level PSNR falls by more than 0.01 dB, so the whole form is held one-sided: no texture more than
   0.05 dB below the plain form (a texture may gain more). The joint pass never leaves the shipped E above where it
   started.
+- The precision switches with the matrix-free conjugate-gradient products (NNTC_B200_OPT_ADJOINT_CG) against the plain
+  form: per-texture PSNR within 0.05 dB.
 - The 4 x 1024 x 1024 material (c0 2, c1 4): the plain form against the reference's own CPU encoder
   (oracle/_ref/nntc_encode_cpu), per-texture PSNR within 0.05 dB.
 - The 4 x 2048 x 1024 material (c0 4, c1 4): against the reference's own CUDA encoder (oracle/_ref/nntc_encode_cuda,
@@ -64,6 +66,18 @@ def test_adjoint_form_vs_plain(index):
         assert adj.e_ship <= adj.e_before_joint * (1 + 1e-12), (adj.e_ship, adj.e_before_joint, adj.joint_taken)
         if adj.joint_taken == 1:
             assert adj.e_joint < adj.e_before_joint
+
+
+@pytest.mark.parametrize("index", [1, 2])
+def test_matrix_free_cg_vs_plain(index):
+    """The precision switches with the conjugate gradients' products matrix-free (the decode's forward pass and its
+    adjoint, no off-diagonal stencil blocks for the CG; the quantised sweeps keep the assembled stencil): per-texture
+    PSNR within 0.05 dB of the plain form."""
+    mat = materials.config(index)
+    nt = len(mat.textures)
+    plain = list(encode(mat, 0).psnr[:nt])
+    free = list(encode(mat, 0, MIXED + (abi.OPT_ADJOINT_CG,)).psnr[:nt])
+    assert all(abs(x - y) <= 0.05 for x, y in zip(free, plain)), (free, plain)
 
 
 def test_config2_plain_vs_reference_cpu(tmp_path):
