@@ -357,8 +357,9 @@ __global__ void __launch_bounds__(OBJ_P_THREADS, 5)
 
 // The mixed-precision objective (the adjoint form): the sites' samples with the float tap rule of the assembly
 // (tap_at, blend), every output row's dot product in FP32 fused multiply-adds with the decoder as a launch parameter,
-// the fractional sites' float targets of the assembly (d->site_tgt), and each residual squared and summed in FP64. E
-// agrees with the FP64 objective to about 1e-7 relative; what decides on E (the stops, the acceptance of a repack pass)
+// the fractional sites' float targets of the assembly (d->site_tgt), each site's squared residuals summed over its
+// outputs in FP32 (a few positive terms) and the sites' sums in FP64. E agrees with the FP64 objective to about 1e-7
+// relative; what decides on E (the stops, the acceptance of a repack pass)
 // sees the same E within tolerances four orders coarser.
 struct ObjDecoderF
 {
@@ -426,16 +427,20 @@ __global__ void __launch_bounds__(OBJ_P_THREADS, 6)
             }
             const float* tg = j == 0 ? V.src + (size_t)local * NOUT
                                      : T.t + (size_t)(T.site0[pl] + local * kc + (j - 1)) * NOUT;
+            // the site's two sums over its outputs in FP32 (NOUT positive terms), each added to the FP64 totals once
+            float sw = 0.0f, ss = 0.0f;
 #pragma unroll
             for (int r = 0; r < NOUT; r++)
             {
-                const double e = (double)(acc[r] - __ldg(tg + r));
-                weighted = fma((double)W.cw[r] * e, e, weighted);
-                if (j == 0)
-                    centre = fma(e, e, centre);
-                else
-                    fractional = fma(e, e, fractional);
+                const float e = acc[r] - __ldg(tg + r);
+                sw = __fmaf_rn(W.cw[r] * e, e, sw);
+                ss = __fmaf_rn(e, e, ss);
             }
+            weighted += (double)sw;
+            if (j == 0)
+                centre += (double)ss;
+            else
+                fractional += (double)ss;
         }
     }
     const double a = block_sum(weighted, red);

@@ -67,3 +67,28 @@ def test_precision_report_against_fp64():
         s.encode(a)
         rep = s.precision_report()
     assert rep["decoder"] <= 1e-4 and rep["level1"] <= 1e-4 and rep["level0"] <= 1e-4, rep
+
+
+@pytest.mark.parametrize("textures,c0,c1,w,h,k", [(4, 4, 4, 128, 96, 4), (6, 4, 4, 70, 52, 4), (2, 2, 4, 64, 48, 2),
+                                                  (3, 3, 2, 45, 31, 1)])
+def test_fp32_objective_vs_fp64(textures, c0, c1, w, h, k):
+    """The adjoint form's objective (the decode in FP32 with fused multiply-adds, each site's squared residuals summed in
+    FP32, the sites' sums in FP64) against the FP64 objective on the same state and decoder: E and every plane's E
+    within 1e-6 relative."""
+    mat, v0, v1 = state(w * h + 7 * textures, w, h, textures, c0, c1, k)
+    rng = np.random.default_rng(w + h)
+    nin, nout = abi.feature_count(c0, c1), 3 * textures
+    with Session(mat) as s:
+        for i in range(len(mat.planes)):
+            s.set_planes(i, v0[i], v1[i])
+        s.set_decoder(rng.standard_normal((nout, nin)) * 0.2, rng.random(nout) * 0.5)
+        out = []
+        for mixed in (0, 1):
+            check(lib().nntc_b200_set_option(s.d, abi.OPT_MIXED_OBJECTIVE, mixed), "option")
+            r = s.objective(k)
+            out.append((r.e, list(r.e_plane[: len(mat.planes)]), r.centre_mse, r.sampled_mse))
+    (e64, p64, c64, s64), (e32, p32, c32, s32) = out
+    assert abs(e32 - e64) <= 1e-6 * e64, (e32, e64)
+    for a, b in zip(p32, p64):
+        assert abs(a - b) <= 1e-6 * b, (a, b)
+    assert abs(c32 - c64) <= 1e-6 * c64 and abs(s32 - s64) <= 1e-6 * max(s64, 1e-300)
