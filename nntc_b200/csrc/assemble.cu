@@ -343,7 +343,16 @@ struct GatherArgs
     long long site0[MAX_PLANES + 1];
     long long bstart[MAX_PLANES + 1];   // each plane's first block
     int slots;            // slots gathered: SLOTS, or 1 for the diagonal blocks and the gradient alone
+    int bc_copy;          // level 0, FP64, for the BC refinement: each block also into the block-major copy
 };
+
+// Where coefficient e of slot `slot` of texel (x, y) sits in the block-major copy: block (y / 4, x / 4) of a plane
+// bx blocks wide, then slot, coefficient and the texel's place in its 4x4 block.
+__device__ __forceinline__ size_t bc_sten_pos(int x, int y, int bx, int slot, int cc, int e)
+{
+    const size_t blk = (size_t)(y >> 2) * bx + (x >> 2);
+    return ((blk * SLOTS + slot) * cc + e) * 16 + (size_t)((y & 3) * 4 + (x & 3));
+}
 
 // The texel at position `pos` of the stencil's colour-major order (the inverse of stencil_pos).
 __device__ __forceinline__ void stencil_texel(long long pos, int w, int h, int& x, int& y)
@@ -427,11 +436,16 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
     const int nbx = tx + ox, nby = ty + oy;
     const size_t T = (size_t)tw_ * th_;
     const int cc = c * c;
+    const bool bc_copy = LEVEL0 && sizeof(TS) == sizeof(double) && A.bc_copy;
     if (nbx < 0 || nbx >= tw_ || nby >= th_)
     {
         // no neighbour in this direction: the reference's block is zero (no site touches both)
         for (int e = 0; e < cc; e++)
+        {
             reinterpret_cast<TS*>(V.stencil)[(size_t)(slot * cc + e) * T + sp] = (TS)0;
+            if (bc_copy)
+                V.bc_sten[bc_sten_pos(tx, ty, (tw_ + 3) >> 2, slot, cc, e)] = 0.0;
+        }
         return;
     }
 
@@ -648,7 +662,11 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
 #pragma unroll
         for (int e = 0; e < PART; e++)
             if (part * PART + e < cc)
+            {
                 reinterpret_cast<TS*>(V.stencil)[(size_t)(slot * cc + part * PART + e) * T + sp] = blk[e];
+                if (bc_copy)
+                    V.bc_sten[bc_sten_pos(tx, ty, (tw_ + 3) >> 2, slot, cc, part * PART + e)] = (double)blk[e];
+            }
     }
     if (LEVEL0)
         store_grad();
@@ -759,6 +777,8 @@ int assemble_split(nntc_b200_device* d, int k, int level0, const Planes& P_texel
         std::memcpy(d->gtab_off[level0], &gt, sizeof(gt));
         d->gtab_kc[level0] = k;
     }
+    G.bc_copy = level0 && !f32 && d->bc_copy ? 1 : 0;
+    d->bc_copied = G.bc_copy && slots == SLOTS;
     G.tab = (const int4*)d->gtab[level0];
     std::memcpy(&G.gt, d->gtab_off[level0], sizeof(G.gt));
     auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };

@@ -317,6 +317,7 @@ struct PlaneView
     double* p;
     double* ap;
     float* prev;        // the plane the stencil was assembled at
+    double* bc_sten;    // level 0 under bc8: the BC refinement's block-major copy of the FP64 stencil
 };
 
 struct Planes

@@ -331,6 +331,7 @@ void layout(nntc_b200_device* d, const nntc_b200_model* m, Carver& take)
         {
             take(p.bc_ep, p.blocks() * m->c0 * 2);
             take(p.bc_sel, p.blocks() * m->c0 * 16);
+            take(p.bc_sten, p.blocks() * SLOTS * m->c0 * m->c0 * 16 * sizeof(double));
         }
     }
     take(d->weights, (size_t)m->nout * m->nin * sizeof(float));

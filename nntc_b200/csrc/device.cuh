@@ -92,6 +92,9 @@ struct DevPlane
     Work work[2];             // [0] level 1 (block b), [1] level 0 (block c', bc8 only)
     uint8_t* bc_ep = nullptr; // blocks * c0 * 2
     uint8_t* bc_sel = nullptr;// blocks * c0 * 16
+    // level 0's FP64 stencil again, block-major for the BC refinement: [block][slot][i][j][texel of the 4x4 block],
+    // written by the assembly the refinement runs on (a block's whole stencil is one contiguous run)
+    double* bc_sten = nullptr;
     size_t blocks() const { return (size_t)((w0 + 3) / 4) * (size_t)((h0 + 3) / 4); }
 };
 
@@ -135,6 +138,8 @@ struct nntc_b200_device
     int gtab_off[2][4][6] = {};          // each table's entry ranges per parity class and slot
     int reference_shaped_assembly = 0;   // 1: the per-texel gather of the reference's shape (same bits, slower)
     int mixed_gram = 0;                  // 1: block (a)'s sums on the tensor cores, BF16 hi + lo (gram_tc.cu)
+    int bc_copy = 0;                     // 1 while the assembly for the BC refinement runs: also write bc_sten
+    int bc_copied = 0;                   // the last such assembly wrote bc_sten itself
     int adjoint_cg = 0;                  // 1: blocks (b) and (c')'s conjugate gradients matrix-free (adjoint_cg.cu)
     int mixed_objective = 0;             // 1: the objective's decode in FP32, its squares summed in FP64
     int mixed_stencil = 0;               // 1: blocks (b) and (c') assemble an FP32 stencil (gathers in FP32)
@@ -233,6 +238,7 @@ inline Planes planes_for(const nntc_b200_device* d, int level0, F items)
         v.p = w.p;
         v.ap = w.ap;
         v.prev = w.prev;
+        v.bc_sten = level0 ? s.bc_sten : nullptr;
         P.start[i] = at;
         const long long n = (long long)items(i);
         at += (n + THREADS - 1) / THREADS * THREADS;

@@ -6,7 +6,9 @@
 // of exact 8-way selector argmins; a step is taken only on a strict decrease weighed in the float arithmetic the
 // file decodes in (src/refine_bc.cu:47-95). Four colours over the block grid keep every block's neighbourhood frozen.
 //
-// B200 shape: ONE WARP PER 4x4 BLOCK, with the block's A2 (up to 64 x 64 doubles) in shared memory. Every value is
+// B200 shape: ONE WARP PER 4x4 BLOCK, with the block's A2 (up to 64 x 64 doubles) in shared memory, read from a
+// block-major copy of the FP64 stencil that the refinement's own assembly writes (a block's coefficients contiguous,
+// so the warp's reads are whole lines instead of scattered doubles of the colour-major stencil). Every value is
 // computed with the arithmetic of the reference's CPU transcription (src/cpu/cpu_refine_bc.cpp:134-400), including
 // its order of summation: each block sum is a SERIAL fold over the sixteen texels in increasing order, which a warp
 // reproduces exactly by shuffling the sixteen per-lane terms to every lane and folding them in texel order. The
@@ -68,7 +70,7 @@ struct BcPlane
     uint8_t* k0;
     double* delta;
     const float* prev;
-    const double* stencil;  // SoA level-0 stencil
+    const double* bsten;    // level 0's FP64 stencil, block-major: [block][slot][i][j][texel of the block]
     const double* grad;
 };
 
@@ -250,12 +252,15 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
     const int gx = R.cx + 2 * (int)(local % cbx);
     const int gy = R.cy + 2 * (int)(local / cbx);
     const int w0 = B.w0, h0 = B.h0;
-    const size_t T = (size_t)w0 * h0;
 
     // The block's quadratic (src/cpu/cpu_refine_bc.cpp:152-205), one lane per row (texel, channel): the row's owned
     // stencil blocks whose partner lies in the block go to S, the rest of the stencil meets the neighbours'
     // corrections in the row's share of A1, summed in the reference's order (per slot: the owned block, then the
-    // neighbour's transposed one).
+    // neighbour's transposed one). The stencil is read from its block-major copy: the block's own coefficients are one
+    // contiguous run (the lanes of one coefficient read consecutive texels), a neighbouring block's transposed ones
+    // the same layout one block over.
+    const size_t gi = (size_t)gy * B.bx + gx;
+    const double* own = B.bsten + gi * (SLOTS * CC * 16);
 #pragma unroll
     for (int q = 0; q < RR; q++)
     {
@@ -266,8 +271,8 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
         const int px = gx * 4 + (t & 3), py = gy * 4 + (t >> 2);
         const bool in = px < w0 && py < h0;
         const size_t ti = in ? (size_t)py * w0 + px : 0;
-        const size_t sp = in ? stencil_pos(px, py, w0, h0) : 0;
         double acc = in ? B.grad[ti * C0 + i] : 0.0;
+#pragma unroll
         for (int slot = 0; slot < SLOTS; slot++)
         {
             int dx, dy;
@@ -276,14 +281,17 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
             const bool f_img = in && fx >= 0 && fx < w0 && fy >= 0 && fy < h0;
             const int lx = fx - gx * 4, ly = fy - gy * 4;
             const bool f_blk = lx >= 0 && lx < 4 && ly >= 0 && ly < 4;
+            const double* row = own + (size_t)(slot * CC + i * C0) * 16 + t;   // coefficient j at row[16 j]
             double* s_row = S + t * TS + slot * CC + i * C0;
+#pragma unroll
             for (int j = 0; j < C0; j++)
-                s_row[j] = f_img && f_blk ? B.stencil[(size_t)(slot * CC + i * C0 + j) * T + sp] : 0.0;
+                s_row[j] = f_img && f_blk ? row[16 * j] : 0.0;
             if (f_img && !f_blk)
             {
                 const double* xn = B.delta + ((size_t)fy * w0 + fx) * C0;
+#pragma unroll
                 for (int j = 0; j < C0; j++)
-                    acc += B.stencil[(size_t)(slot * CC + i * C0 + j) * T + sp] * xn[j];
+                    acc += row[16 * j] * xn[j];
             }
             if (slot == 0 || !in)
                 continue;
@@ -291,15 +299,17 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS, 8) k_bc_refine(BcPlanes P, 
             const int mx = ax - gx * 4, my = ay - gy * 4;
             if (ax < 0 || ax >= w0 || ay < 0 || ay >= h0 || (mx >= 0 && mx < 4 && my >= 0 && my < 4))
                 continue;
-            const size_t nt = (size_t)ay * w0 + ax, np = stencil_pos(ax, ay, w0, h0);
+            const size_t nt = (size_t)ay * w0 + ax;
+            const size_t nb = (size_t)(ay >> 2) * B.bx + (size_t)(ax >> 2);
+            const double* col = B.bsten + ((nb * SLOTS + slot) * CC + i) * 16 + (size_t)((ay & 3) * 4 + (ax & 3));
             const double* xn = B.delta + nt * C0;
+#pragma unroll
             for (int j = 0; j < C0; j++)
-                acc += B.stencil[(size_t)(slot * CC + j * C0 + i) * T + np] * xn[j];
+                acc += col[(size_t)16 * C0 * j] * xn[j];   // coefficient (j, i) of the neighbour's block
         }
         a1[r] = acc;
         dv[r] = in ? (double)B.v0[ti * C0 + i] - (double)B.prev[ti * C0 + i] : 0.0;
     }
-    const size_t gi = (size_t)gy * B.bx + gx;
     if (lane < C0)
     {
         s_ep[2 * lane] = B.ep[(gi * C0 + lane) * 2];
@@ -572,7 +582,7 @@ static BcPlanes bc_planes(nntc_b200_device* d, F items)
         b.k0 = s.k0;
         b.delta = s.work[1].x;
         b.prev = s.work[1].prev;
-        b.stencil = s.work[1].stencil;
+        b.bsten = s.bc_sten;
         b.grad = s.work[1].grad;
         P.start[i] = at;
         at += (long long)items(i);

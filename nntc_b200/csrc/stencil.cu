@@ -1263,6 +1263,25 @@ int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, doub
     return NNTC_B200_OK;
 }
 
+// Level 0's stencil copied into the BC refinement's block-major layout (bc_sten: [block][slot][i][j][texel of the
+// block]), one thread per texel; used when the assembly did not write the copy itself.
+__global__ void k_bc_sten_copy(Planes P)
+{
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    const int pl = plane_of(P, base);
+    const PlaneView& V = P.p[pl];
+    const long long t = base - P.start[pl] + threadIdx.x;
+    if (t >= (long long)V.w * V.h)
+        return;
+    const int x = (int)(t % V.w), y = (int)(t / V.w), cc = P.c * P.c;
+    const size_t T = (size_t)V.w * V.h, sp = stencil_pos(x, y, V.w, V.h);
+    const size_t blk = (size_t)(y >> 2) * (size_t)((V.w + 3) >> 2) + (size_t)(x >> 2);
+    const int in = (y & 3) * 4 + (x & 3);
+    for (int slot = 0; slot < SLOTS; slot++)
+        for (int e = 0; e < cc; e++)
+            V.bc_sten[((blk * SLOTS + slot) * cc + e) * 16 + in] = V.stencil[(size_t)(slot * cc + e) * T + sp];
+}
+
 // Block (c')'s assembly alone with no ridge, the correction measured from the plane as it stands (for refine_bc). The
 // refinement's decisions are the reference's on an FP64 stencil, so this assembly is FP64 in either form.
 int assemble_for_refine(nntc_b200_device* d, const nntc_b200_model* m, int k, double* ms)
@@ -1271,12 +1290,24 @@ int assemble_for_refine(nntc_b200_device* d, const nntc_b200_model* m, int k, do
     {
         nntc_b200_device* d;
         int was;
-        ~Fp64Scope() { d->mixed_stencil = was; }
+        ~Fp64Scope()
+        {
+            d->mixed_stencil = was;
+            d->bc_copy = 0;
+        }
     } fp64{ d, d->mixed_stencil };
     d->mixed_stencil = 0;
+    d->bc_copy = 1;   // the refinement reads the block-major copy the gather writes beside the stencil
+    d->bc_copied = 0;
     NB_TRY(block_begin(d));
     NB_TRY(assemble(d, m, k, 0.0, 1));
     Planes P = texel_planes(d, 1, k);
+    if (!d->bc_copied)
+    {
+        // the reference-shaped assembly wrote the stencil alone: the copy from it
+        k_bc_sten_copy<<<(int)(P.start[P.n] / THREADS), THREADS, 0, d->stream>>>(P);
+        NB_LAUNCHED();
+    }
     k_snapshot<<<(int)(P.start[P.n] / THREADS), THREADS, 0, d->stream>>>(P);
     NB_LAUNCHED();
     return block_end(d, ms);
