@@ -476,16 +476,18 @@ _PIX3 = 2796160
 TRAFFIC_PER_UNIT = {
     "adjoint": {
         "normal_equations": (723597056 + 8700928) / _PIX3,                    # k_ls_accumulate_tc<12>
-        "objective": (718757888 + 4184064) / _PIX3,                           # k_objective_f32<12>
-        "assemble_level0": (718829056 + 627887616 + 671612160 + 943460608) / _PIX3,
+        "objective": (718641152 + 4395008) / _PIX3,                           # k_objective_f32<12>
+        "assemble_level0": (718829056 + 627887616 + 671188992 + 944002048) / _PIX3,
         "assemble_level1": (718788608 + 627927552 + 885506560 + 71808000) / _PIX3,
         "quant_sweep": (608629248 + 41608448) / _PIX3,                        # a level-0 colour launch
-        "bc_refine": (1151548000 + 42135040) / _PIX3,                         # one colour
+        "bc_refine": (1279862000 + 43057664) / _PIX3,                         # one colour
     },
     "plain": {
         "normal_equations": (722979328 + 8198656) / _PIX3,                    # k_ls_accumulate_mma<12>
+        "objective": (1255526000 + 4267264) / _PIX3,                          # k_objective_p<12>
+        "assemble_level0": (718652928 + 626347520 + 671268096 + 1827433000) / _PIX3,
         "quant_sweep": (1030932000 + 46642944) / _PIX3,
-        "bc_refine": (1151548000 + 42135040) / _PIX3,
+        "bc_refine": (1279862000 + 43057664) / _PIX3,
     },
 }
 
@@ -496,8 +498,7 @@ BINDING = {
         "assemble_level1": "issue: the fused FP32 site terms at ~88% issue; the gather at ~50% issue (cp.async ring)",
         "objective": "issue: FP32 decode with fused multiply-adds, ~72% issue, FP32 pipe ~36%",
         "normal_equations": "latency of the site rows' loads at 12 warps per SM; the tensor pipe (tcgen05) ~14% busy",
-        "bc_refine": "latency: the set-up's scattered stencil reads (~2.3x the needed bytes), then the ordered "
-                     "selector steps",
+        "bc_refine": "latency: the set-up (block-major stencil copy, coalesced), then the ordered selector steps",
         "quant_sweep": "HBM (FP32 stencil, a level-0 colour at ~62% of the copy bandwidth)",
         "cg_product_level0": "HBM (FP32 stencil)",
         "cg_product_level1": "DRAM latency (small launches)",
@@ -508,8 +509,7 @@ BINDING = {
         "assemble_level1": "FP32/ALU issue (site terms) and L2 latency (gather)",
         "objective": "FP64 pipe (~50% of peak)",
         "normal_equations": "the FP64 tensor pipe (mma.sync m8n8k4, ~76% busy)",
-        "bc_refine": "latency: the set-up's scattered stencil reads (~2.3x the needed bytes), then the ordered "
-                     "selector steps",
+        "bc_refine": "latency: the set-up (block-major stencil copy, coalesced), then the ordered selector steps",
         "quant_sweep": "HBM (FP64 stencil, a level-0 colour at ~78% of the copy bandwidth)",
         "cg_product_level0": "HBM (FP64 stencil)",
         "cg_product_level1": "DRAM latency (small launches)",
