@@ -442,7 +442,7 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
         // no neighbour in this direction: the reference's block is zero (no site touches both)
         for (int e = 0; e < cc; e++)
         {
-            reinterpret_cast<TS*>(V.stencil)[(size_t)(slot * cc + e) * T + sp] = (TS)0;
+            reinterpret_cast<TS*>(V.stencil)[sten_index<TS>(slot, e, cc, T, sp)] = (TS)0;
             if (bc_copy)
                 V.bc_sten[bc_sten_pos(tx, ty, (tw_ + 3) >> 2, slot, cc, e)] = 0.0;
         }
@@ -659,11 +659,24 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
                 if (part * PART + e < cc)
                     blk[e] += s * mono_entry<TS>(A, L, part * PART + e);
         }
+        if constexpr (sizeof(TS) == sizeof(float))
+        {
+            // the FP32 stencil keeps a texel's block contiguous: whole 16-byte stores when the block is 16 floats
+            if (cc == MAX_CH * MAX_CH)
+            {
+                float4* out = reinterpret_cast<float4*>(reinterpret_cast<float*>(V.stencil) +
+                                                        sten_index<float>(slot, part * PART, cc, T, sp));
+#pragma unroll
+                for (int v = 0; v < PART / 4; v++)
+                    out[v] = make_float4(blk[4 * v], blk[4 * v + 1], blk[4 * v + 2], blk[4 * v + 3]);
+                continue;
+            }
+        }
 #pragma unroll
         for (int e = 0; e < PART; e++)
             if (part * PART + e < cc)
             {
-                reinterpret_cast<TS*>(V.stencil)[(size_t)(slot * cc + part * PART + e) * T + sp] = blk[e];
+                reinterpret_cast<TS*>(V.stencil)[sten_index<TS>(slot, part * PART + e, cc, T, sp)] = blk[e];
                 if (bc_copy)
                     V.bc_sten[bc_sten_pos(tx, ty, (tw_ + 3) >> 2, slot, cc, part * PART + e)] = (double)blk[e];
             }

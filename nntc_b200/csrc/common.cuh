@@ -270,6 +270,16 @@ __host__ __device__ __forceinline__ size_t stencil_pos(int x, int y, int w, int 
     return base + (size_t)(y >> 1) * (cx ? w1c : w0c) + (size_t)(x >> 1);
 }
 
+// Where coefficient e (= i C + j) of owned slot `slot` of the texel at stencil position sp sits in a stored stencil of
+// T texels. FP64 (the plain form): structure of arrays, [slot][e][texel], one plane per coefficient. FP32 (the adjoint
+// form): [slot][texel][e], a texel's C x C block of one slot contiguous, so a thread reads a block as whole 16-byte
+// vectors and a warp's 32 blocks as one contiguous run.
+template <typename TS>
+__host__ __device__ __forceinline__ size_t sten_index(int slot, int e, int cc, size_t T, size_t sp)
+{
+    return sizeof(TS) == sizeof(double) ? (size_t)(slot * cc + e) * T + sp : ((size_t)slot * T + sp) * cc + (size_t)e;
+}
+
 // The floor halving of a mip chain, never below one texel (src/image.h:335-338).
 __host__ __device__ __forceinline__ int mip_dim(int n)
 {

@@ -891,11 +891,14 @@ int nntc_b200_probe_workspace(nntc_b200_device* d, int plane, int level0, double
         std::vector<double> soa(t * per);
         if (d->sten_f32[level0 ? 1 : 0])
         {
-            // an FP32 stencil (the adjoint form's), widened
+            // an FP32 stencil (the adjoint form's, [slot][texel][e]), widened into the SoA order
             std::vector<float> f(t * per);
             NB_TRY(download(d, f.data(), w.stencil, f.size() * sizeof(float)));
-            for (size_t q = 0; q < f.size(); q++)
-                soa[q] = (double)f[q];
+            const int cc = (int)(c * c);
+            for (int slot = 0; slot < SLOTS; slot++)
+                for (size_t at = 0; at < t; at++)
+                    for (int e = 0; e < cc; e++)
+                        soa[(size_t)(slot * cc + e) * t + at] = (double)f[sten_index<float>(slot, e, cc, t, at)];
         }
         else
             NB_TRY(download(d, soa.data(), w.stencil, soa.size() * sizeof(double)));

@@ -367,6 +367,43 @@ __device__ __forceinline__ double sten(const PlaneView& V, size_t idx)
     return (double)reinterpret_cast<const TS*>(V.stencil)[idx];
 }
 
+// A texel's C x C block of slot `slot` (the texel at stencil position sp). An FP32 block of 16 (or 4) coefficients is
+// read at once as 16-byte vector loads into registers; an FP64 block (and any other) is read a coefficient at a time
+// where it is used, as the plain form always has (holding 16 doubles would cost its kernels occupancy).
+template <int C, typename TS>
+struct StenBlock
+{
+    static constexpr int cc = C * C;
+    static constexpr bool vec = sizeof(TS) == sizeof(float) && cc % 4 == 0;
+    float f[vec ? cc : 1];
+    const TS* base;
+    size_t T, sp;
+    int slot;
+    __device__ __forceinline__ StenBlock(const PlaneView& V, int slot_, size_t T_, size_t sp_)
+        : base(reinterpret_cast<const TS*>(V.stencil)), T(T_), sp(sp_), slot(slot_)
+    {
+        if constexpr (vec)
+        {
+            const float4* q = reinterpret_cast<const float4*>(base + ((size_t)slot * T + sp) * cc);
+#pragma unroll
+            for (int v = 0; v < cc / 4; v++)
+            {
+                const float4 x = __ldg(q + v);
+                f[4 * v] = x.x;
+                f[4 * v + 1] = x.y;
+                f[4 * v + 2] = x.z;
+                f[4 * v + 3] = x.w;
+            }
+        }
+    }
+    __device__ __forceinline__ double operator[](int e) const
+    {
+        if constexpr (vec)
+            return (double)f[e];
+        else
+            return (double)base[sten_index<TS>(slot, e, cc, T, sp)];
+    }
+};
 
 // ---- ridge, preconditioner ----------------------------------------------------------------------------------------
 
@@ -385,7 +422,7 @@ __global__ void __launch_bounds__(THREADS) k_diag(Planes P, Red R)
     if (t < (long long)T)
         for (int a = 0; a < c; a++)
         {
-            const double x = sten<TS>(V, (size_t)(a * c + a) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h));
+            const double x = sten<TS>(V, sten_index<TS>(0, a * c + a, c * c, T, stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)));
             v[0] += x;
             v[1] = x < v[1] ? x : v[1];
             v[2] = x > v[2] ? x : v[2];
@@ -486,13 +523,14 @@ __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long
     const int tx = (int)(t % V.w), ty = (int)(t / V.w);
     const size_t sp = stencil_pos(tx, ty, V.w, V.h);
     const double* xt = x + (size_t)t * C;
+    const StenBlock<C, TS> self(V, 0, T, sp);
 #pragma unroll
     for (int i = 0; i < C; i++)
     {
         double s = lambda * xt[i];
 #pragma unroll
         for (int j = 0; j < C; j++)
-            s += sten<TS>(V, (size_t)(i * C + j) * T + sp) * xt[j];
+            s += self[i * C + j] * xt[j];
         acc[i] = s;
     }
     // Every neighbour's loads are issued whether or not the neighbour exists (from a clamped, in-range texel), and a
@@ -507,12 +545,13 @@ __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long
         const bool fwd = fx >= 0 && fx < V.w && fy >= 0 && fy < V.h;
         const int gx = fwd ? fx : tx, gy = fwd ? fy : ty;
         const double* xn = x + ((size_t)gy * V.w + gx) * C;
+        const StenBlock<C, TS> blk(V, slot, T, sp);
 #pragma unroll
         for (int i = 0; i < C; i++)
 #pragma unroll
             for (int j = 0; j < C; j++)
             {
-                const double e = sten<TS>(V, (size_t)(slot * cc + i * C + j) * T + sp) * xn[j];
+                const double e = blk[i * C + j] * xn[j];
                 acc[i] += fwd ? e : -0.0;
             }
         const int bx = tx - dx, by = ty - dy;
@@ -520,12 +559,13 @@ __device__ __forceinline__ void stencil_apply(const PlaneView& V, size_t T, long
         const int hx = bwd ? bx : tx, hy = bwd ? by : ty;
         const size_t nt = (size_t)hy * V.w + hx, np = stencil_pos(hx, hy, V.w, V.h);
         const double* xb = x + nt * C;
+        const StenBlock<C, TS> nbk(V, slot, T, np);
 #pragma unroll
         for (int i = 0; i < C; i++)
 #pragma unroll
             for (int j = 0; j < C; j++)
             {
-                const double e = sten<TS>(V, (size_t)(slot * cc + j * C + i) * T + np) * xb[j];
+                const double e = nbk[j * C + i] * xb[j];
                 acc[i] += bwd ? e : -0.0;
             }
     }
@@ -549,7 +589,7 @@ __global__ void __launch_bounds__(THREADS) k_precondition_init(Planes P, Red R)
         double a[MAX_CH * MAX_CH], inv[MAX_CH * MAX_CH];
         for (int i = 0; i < c; i++)
             for (int j = 0; j < c; j++)
-                a[i * c + j] = sten<TS>(V, (size_t)(i * c + j) * T + stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h)) +
+                a[i * c + j] = sten<TS>(V, sten_index<TS>(0, i * c + j, c * c, T, stencil_pos((int)(t % V.w), (int)(t / V.w), V.w, V.h))) +
                                (i == j ? lambda : 0.0);
         if (!invert(a, c, inv))
             for (int i = 0; i < c; i++)
@@ -902,12 +942,13 @@ __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
         const bool fwd = fx >= 0 && fx < V.w && fy >= 0 && fy < V.h;
         const int gx = fwd ? fx : tx, gy = fwd ? fy : ty;
         const double* xn = V.x + ((size_t)gy * V.w + gx) * c;
+        const StenBlock<C, TS> blk(V, slot, T, sp);
 #pragma unroll
         for (int i = 0; i < c; i++)
 #pragma unroll
             for (int j = 0; j < c; j++)
             {
-                const double e = sten<TS>(V, (size_t)(slot * cc + i * c + j) * T + sp) * xn[j];
+                const double e = blk[i * c + j] * xn[j];
                 nb[i] += fwd ? e : -0.0;
             }
         const int bx = tx - dx, by = ty - dy;
@@ -915,29 +956,31 @@ __global__ void __launch_bounds__(THREADS) k_quant_sweep(Planes P, SweepArgs A)
         const int hx = bwd ? bx : tx, hy = bwd ? by : ty;
         const size_t nt = (size_t)hy * V.w + hx, np = stencil_pos(hx, hy, V.w, V.h);
         const double* xb = V.x + nt * c;
+        const StenBlock<C, TS> nbk(V, slot, T, np);
 #pragma unroll
         for (int i = 0; i < c; i++)
 #pragma unroll
             for (int j = 0; j < c; j++)
             {
-                const double e = sten<TS>(V, (size_t)(slot * cc + j * c + i) * T + np) * xb[j];
+                const double e = nbk[j * c + i] * xb[j];
                 nb[i] += bwd ? e : -0.0;
             }
     }
+    const StenBlock<C, TS> self(V, 0, T, sp);
     unsigned int changed = 0;
 #pragma unroll
     for (int q = 0; q < c; q++)
     {
         const size_t idx = t * c + q;
         const float l = A.lo[q], span = A.hi[q] - A.lo[q];
-        const double a = sten<TS>(V, (size_t)(q * c + q) * T + sp) + lambda;
+        const double a = self[q * c + q] + lambda;
         if (!(a > 0.0) || !(span > 0.0f))
             continue;
         double rest = nb[q];
 #pragma unroll
         for (int j = 0; j < c; j++)
             if (j != q)
-                rest += sten<TS>(V, (size_t)(q * c + j) * T + sp) * V.x[t * c + j];
+                rest += self[q * c + j] * V.x[t * c + j];
         const double b = V.grad[idx] + rest;
         const double want = (double)V.prev[idx] - b / a;
         const int kk = grid_index(l, A.hi[q], A.bits, (float)want);
