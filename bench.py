@@ -479,7 +479,7 @@ TRAFFIC_PER_UNIT = {
         "objective": (718641152 + 4395008) / _PIX3,                           # k_objective_f32<12>
         "assemble_level0": (718829056 + 627887616 + 671188992 + 944002048) / _PIX3,
         "assemble_level1": (718788608 + 627927552 + 885506560 + 71808000) / _PIX3,
-        "quant_sweep": (608629248 + 41608448) / _PIX3,                        # a level-0 colour launch
+        "quant_sweep": (610947328 + 42693888) / _PIX3,                        # a level-0 colour launch
         "bc_refine": (1279862000 + 43057664) / _PIX3,                         # one colour
     },
     "plain": {
@@ -499,7 +499,7 @@ BINDING = {
         "objective": "issue: FP32 decode with fused multiply-adds, ~72% issue, FP32 pipe ~36%",
         "normal_equations": "latency of the site rows' loads at 12 warps per SM; the tensor pipe (tcgen05) ~14% busy",
         "bc_refine": "latency: the set-up (block-major stencil copy, coalesced), then the ordered selector steps",
-        "quant_sweep": "HBM (FP32 stencil, a level-0 colour at ~62% of the copy bandwidth)",
+        "quant_sweep": "HBM (FP32 per-block stencil, a level-0 colour at ~67% of the copy bandwidth)",
         "cg_product_level0": "HBM (FP32 stencil)",
         "cg_product_level1": "DRAM latency (small launches)",
     },
