@@ -497,7 +497,7 @@ BINDING = {
         "assemble_level0": "issue: the fused FP32 site terms at ~88% issue; the gather's L2 latency (one visit ahead)",
         "assemble_level1": "issue: the fused FP32 site terms at ~88% issue; the gather at ~50% issue (cp.async ring)",
         "objective": "issue: FP32 decode with fused multiply-adds, ~72% issue, FP32 pipe ~36%",
-        "normal_equations": "latency of the site rows' loads at 12 warps per SM; the tensor pipe (tcgen05) ~14% busy",
+        "normal_equations": "latency of the site rows' loads at 16 warps per SM; the tensor pipe (tcgen05) ~14% busy",
         "bc_refine": "latency: the set-up (block-major stencil copy, coalesced), then the ordered selector steps",
         "quant_sweep": "HBM (FP32 per-block stencil, a level-0 colour at ~67% of the copy bandwidth)",
         "cg_product_level0": "HBM (FP32 stencil)",

@@ -29,10 +29,12 @@
 // every byte the MMAs can address under either reading of the two strides lies inside the CTA's shared memory
 // (checked at compile time below).
 //
-// The tensor-core plumbing, all by inline PTX: tcgen05.alloc / dealloc of 128 TMEM columns per CTA (three CTAs per SM
-// by shared memory, 384 of the 512 columns, so an allocation never waits on another CTA), shared-memory matrix
+// The tensor-core plumbing, all by inline PTX: tcgen05.alloc / dealloc of 128 TMEM columns per CTA (at most four CTAs
+// per SM by shared memory and registers, 512 of the 512 columns, so an allocation never waits on another CTA),
+// shared-memory matrix
 // descriptors, tcgen05.mma.cta_group::1.kind::f16 issued by one thread, tcgen05.commit to an mbarrier per operand
-// buffer (two buffers: one stage's MMAs run while the next stage's rows are formed), tcgen05.ld of 32 lanes x 32
+// buffer (one buffer: the next stage's rows are formed in registers while the stage's MMAs run, and stored once they
+// are done; a second buffer measured slower, costing the fourth CTA per SM), tcgen05.ld of 32 lanes x 32
 // columns per warp. No TMA, no multicast, no cluster: the operands are computed by the threads, not copied. Every wait
 // on an mbarrier is bounded; a wait that gives up raises the device status word, waits (bounded) once more, frees the
 // tensor memory and leaves.
@@ -50,7 +52,7 @@ namespace nb
 constexpr int TG_THREADS = 128;                    // four warps; a thread's texel, and TMEM lane = row of D
 constexpr int TG_SITES = 128;                      // sites per stage
 constexpr int TG_KSTEPS = TG_SITES / 16;           // MMAs per stage
-constexpr int TG_BUFFERS = 2;                      // operand buffers
+constexpr int TG_BUFFERS = 1;                      // operand buffers
 constexpr int TG_STAGES_PER_BATCH = 2;             // FP32 accumulation spans 256 sites (512 measured
                                                    // 5x the decoder error at a converged state)
 constexpr uint32_t TG_CORE = 128;                  // one core matrix: 8 sites x 8 rows of bf16
@@ -71,7 +73,7 @@ constexpr uint32_t TG_WAIT_LIMIT = 1u << 26;
 constexpr uint32_t TG_MAX_STRIDE = TG_MN > TG_KG ? TG_MN : TG_KG;
 constexpr uint32_t TG_REACH = (TG_BUFFERS - 1) * TG_BUF + (TG_KSTEPS - 1) * TG_STEP + 16 * TG_MAX_STRIDE + 16;
 constexpr uint32_t TG_SHARED = TG_ACC_OFFSET + TG_ACC_BYTES > TG_REACH ? TG_ACC_OFFSET + TG_ACC_BYTES : TG_REACH;
-static_assert(TG_SHARED <= 76 * 1024, "three CTAs per SM");
+static_assert(TG_SHARED <= 56 * 1024, "four CTAs per SM");
 static_assert(TG_ACC_OFFSET % 16 == 0 && TG_BUF % 16 == 0, "16-byte aligned operand and accumulator regions");
 
 struct TcArgs
@@ -175,7 +177,7 @@ __device__ __forceinline__ void tc_readback(uint32_t tmem, int warp, int lane, d
 }
 
 template <int NOUT>
-__global__ void __launch_bounds__(TG_THREADS, 3) k_ls_accumulate_tc(Planes P, const __grid_constant__ TcArgs A)
+__global__ void __launch_bounds__(TG_THREADS, 4) k_ls_accumulate_tc(Planes P, const __grid_constant__ TcArgs A)
 {
     extern __shared__ __align__(1024) unsigned char tg_sh[];
     unsigned char* tiles = tg_sh;
