@@ -375,7 +375,7 @@ struct ObjTargetsF
 };
 
 template <int NOUT>
-__global__ void __launch_bounds__(OBJ_P_THREADS, 6)
+__global__ void __launch_bounds__(OBJ_P_THREADS, 8)
     k_objective_f32(Planes P, ObjDecoderF W, double* partial, const __grid_constant__ ObjTargetsF T)
 {
     __shared__ double red[32];
