@@ -301,7 +301,9 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
             (copy ? copies : order).push_back(s2);
         }
         order.insert(order.end(), copies.begin(), copies.end());
-        std::vector<int> chosen(order.begin(), order.begin() + taken);
+        std::vector<int> chosen((size_t)taken);
+        for (int c = 0; c < taken; c++)
+            chosen[(size_t)c] = order[(size_t)c];
         std::sort(chosen.begin(), chosen.end());
         bool plain = true;
         for (int c = 0; c < taken; c++)
@@ -355,15 +357,21 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     NB_TRY(objective(e));
     r->e_init = e.e;
     NB_TRY(block_a());
-    NB_TRY(objective(e));
+    // E between the init's steps is the reference's report and decides nothing until the last one, which the first
+    // round's stop test compares against; the adjoint form leaves the others out, the plain form keeps them
+    const bool seeding = m->init0_residual && m->c0 > 0;
+    if (a->form == 0 || !seeding)
+        NB_TRY(objective(e));
     if (m->init0_residual)
         for (int c = 0; c < m->c0; c++)
         {
             nntc_b200_init0_report crep{};
             NB_TRY(nntc_b200_init0_residual_channel(d, m, c, per_site, &crep, nullptr));
-            NB_TRY(objective(e));
+            if (a->form == 0)
+                NB_TRY(objective(e));
             NB_TRY(block_a());
-            NB_TRY(objective(e));
+            if (a->form == 0 || c == m->c0 - 1 || !bc8)
+                NB_TRY(objective(e));
             if (!bc8)
             {
                 std::vector<nntc_b200_level0_report> l0((size_t)np);
