@@ -105,9 +105,9 @@ int joint_pass(nntc_b200_device* d, nntc_b200_model* m, const nntc_b200_encode_a
     };
     NB_TRY(nb::descent_direction(d, m, k, a->ridge, 0));
     NB_TRY(nb::descent_direction(d, m, k, a->ridge, 1));
+    // the pass starts from the shipped state, whose E the caller measured (e_ship)
     nntc_b200_objective e{};
-    NB_TRY(objective(e));
-    double best_e = e.e;
+    double best_e = e_ship;
     float best = 0.0f;
     // the step lengths tried with the decoder held (E alone decides among them); the decoder is re-solved once, at
     // the step taken
