@@ -24,7 +24,7 @@ namespace nb
 {
 
 int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries,
-                            const SiteTargetView& tgt, cudaStream_t stream);
+                            const SiteTargetView& tgt, cudaStream_t stream, double* obj_partial);
 int ensure_site_targets(nntc_b200_device* d, int k, int level0);
 
 struct LsArgs
@@ -187,7 +187,21 @@ __global__ void k_ls_reduce(const double* partial, int entries, int planes, cons
     out[e] = total;
 }
 
-int normal_equations(nntc_b200_device* d, int k, const double* per_site, double* ms)
+// Each plane's three objective sums from the normal equations' pass, its CTAs' partials added in block order.
+__global__ void k_ls_obj_reduce(const double* partial, int planes, double* out)
+{
+    const int pl = blockIdx.x, q = threadIdx.x;
+    if (pl >= planes || q >= 3)
+        return;
+    double t = 0.0;
+    for (int b = 0; b < LS_GRID; b++)
+        t += partial[((size_t)pl * 3 + q) * LS_GRID + b];
+    out[3 * pl + q] = t;
+}
+
+// obj_sums (the mixed-precision Gram only): also the objective's three raw sums per plane of the decoder on the device,
+// at the same sites, into host memory (3 per plane).
+int normal_equations(nntc_b200_device* d, int k, const double* per_site, double* ms, std::vector<double>* obj_sums)
 {
     const int mm = d->nin + 1;
     const int entries = mm * (mm + 1) / 2 + d->nout * mm;
@@ -211,7 +225,7 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     {
         NB_CUDA(cudaMemsetAsync(d->counters + CNT_STATUS, 0, sizeof(unsigned int), d->stream));
         NB_TRY(ktimer_begin(d, NNTC_B200_K_NORMAL_EQ));
-        NB_TRY(launch_ls_accumulate_tc(d, P, d->ls_partial, entries, A.tgt, d->stream));
+        NB_TRY(launch_ls_accumulate_tc(d, P, d->ls_partial, entries, A.tgt, d->stream, obj_sums ? d->ls_obj : nullptr));
         NB_TRY(ktimer_end(d));
     }
     else
@@ -244,7 +258,24 @@ int normal_equations(nntc_b200_device* d, int k, const double* per_site, double*
     k_ls_reduce<<<grid_for((size_t)entries, 128), 128, 0, d->stream>>>(d->ls_partial, entries, P.n, omega,
                                                                       d->reduction);
     NB_LAUNCHED();
+    const bool with_obj = obj_sums && d->mixed_gram;
+    double* obj_out = d->ls_obj + (size_t)P.n * 3 * LS_GRID;
+    if (with_obj)
+    {
+        k_ls_obj_reduce<<<P.n, 32, 0, d->stream>>>(d->ls_obj, P.n, obj_out);
+        NB_LAUNCHED();
+    }
     NB_TRY(block_end(d, ms));
+    if (with_obj)
+    {
+        obj_sums->assign((size_t)3 * P.n, 0.0);
+        NB_TRY(download(d, obj_sums->data(), obj_out, obj_sums->size() * sizeof(double)));
+    }
+    else if (obj_sums)
+    {
+        set_error(NNTC_B200_ERR_STATE, "the objective rides only on the tensor-core normal equations");
+        return NNTC_B200_ERR_STATE;
+    }
     if (d->mixed_gram)
     {
         unsigned int status = 0;
@@ -507,6 +538,9 @@ static_assert(sizeof(DecoderSolveOut) <= 2048, "the arena's dec_solve slice hold
 
 static long long g_rung_tally[4] = { 0, 0, 0, 0 };
 
+void objective_from_sums(const nntc_b200_model& m, int k, const double* per_site, const std::vector<double>& acc,
+                         nntc_b200_objective* r);
+
 int solve_decoder_on_device(nntc_b200_device* d, nntc_b200_model& m, int k, const double* per_site)
 {
     DecoderSolveArgs a{};
@@ -556,13 +590,43 @@ extern "C"
 int nntc_b200_solve_decoder(nntc_b200_device* d, nntc_b200_model* m, int k, const double* per_site, double* ms)
 {
     double t = 0.0;
-    NB_TRY(normal_equations(d, k, per_site, &t));
+    NB_TRY(normal_equations(d, k, per_site, &t, nullptr));
     NB_TRY(solve_decoder_on_device(d, *m, k, per_site));
     NB_TRY(upload_decoder(d, m));
     if (ms)
         *ms = t;
     return NNTC_B200_OK;
 }
+
+}   // extern "C"
+
+namespace nb
+{
+
+// The adjoint form's closing pass of a round: block (a)'s normal equations at the current latents (kept on the device
+// for the next round's solve) and E of the current decoder at the same sites, from one pass over the sites.
+int normal_equations_and_objective(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                                   nntc_b200_objective* e, double* ms)
+{
+    std::vector<double> sums;
+    NB_TRY(normal_equations(d, k, per_site, ms, &sums));
+    objective_from_sums(*m, k, per_site, sums, e);
+    if (ms)
+        e->ms = *ms;
+    return NNTC_B200_OK;
+}
+
+// Block (a) from the normal equations already on the device (normal_equations_and_objective at the same latents).
+int solve_decoder_prepared(nntc_b200_device* d, nntc_b200_model* m, int k, const double* per_site)
+{
+    NB_TRY(solve_decoder_on_device(d, *m, k, per_site));
+    return upload_decoder(d, m);
+}
+
+}   // namespace nb
+
+extern "C"
+{
 
 void nntc_b200_decoder_ridge_tally(long long out[4])
 {

@@ -371,6 +371,7 @@ void layout(nntc_b200_device* d, const nntc_b200_model* m, Carver& take)
     take(d->gtab[1], (size_t)GATHER_TABLE_MAX * 16);
     // the objective's partials: two triples per 256-pixel block (its blocks are 128 threads), then three sums per plane
     take(d->obj_partial, (2 * blocks * 3 + 3 * MAX_PLANES) * sizeof(double));
+    take(d->ls_obj, (d->planes.size() * 3 * LS_GRID + 3 * MAX_PLANES) * sizeof(double));
     d->scratch_floats = std::max(max0 * (size_t)m->c0, max1 * (size_t)m->c1);
     d->scratch_bytes = d->scratch_floats;
     take(d->scratch, d->scratch_floats * sizeof(float));

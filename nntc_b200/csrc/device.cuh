@@ -124,6 +124,7 @@ struct nntc_b200_device
     void* dec_solve = nullptr;           // the device decoder solve's answer: the rung and the decoder (2 KB)
     double* ls_partial = nullptr;        // planes * entries * LS_GRID, then one weight per plane
     double* obj_partial = nullptr;       // 3 * MAX_PLANES * OBJ_GRID
+    double* ls_obj = nullptr;            // planes * 3 * LS_GRID: the objective sums the normal equations' pass forms
     double* bc_stats = nullptr;          // MAX_PLANES * 2
     unsigned int* radix = nullptr;       // 2 * MAX_CH * 2048 words: the grid fit's histograms and flags
     double* site_terms = nullptr;        // every site's gradient term of the assembly, max(C0, C1) per site at K = 4

@@ -56,6 +56,9 @@ namespace nb
 int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0);
 int joint_apply(nntc_b200_device* d, const nntc_b200_model* m, int k, int level0, float alpha);
 int psnr_base(nntc_b200_device* d, const nntc_b200_model* m, double* psnr);
+int normal_equations_and_objective(nntc_b200_device* d, const nntc_b200_model* m, int k, const double* per_site,
+                                   nntc_b200_objective* e, double* ms);
+int solve_decoder_prepared(nntc_b200_device* d, nntc_b200_model* m, int k, const double* per_site);
 }
 
 namespace
@@ -387,10 +390,19 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
     bool frozen = false;
     int tol_hits = 0;
     double e_prev = e.e;
+    // the adjoint form closes a round with one pass that forms E and the next round's normal equations together (same
+    // sites, same latents): `prepared` says the device holds those normal equations for the next block (a)
+    bool prepared = false;
     for (int round = 1; round <= a->rounds; round++)
     {
         nntc_b200_objective ea{}, eb{}, ec{};
-        NB_TRY(block_a());
+        if (prepared)
+        {
+            NB_TRY(nb::solve_decoder_prepared(d, m, k, per_site));
+            prepared = false;
+        }
+        else
+            NB_TRY(block_a());
         // E after blocks (a) and (b) is the reference's report (src/main.cpp's per-block lines) and decides nothing;
         // the adjoint form leaves it out, the plain form keeps the reference's passes
         if (a->form == 0)
@@ -435,7 +447,15 @@ int nntc_b200_encode_on_device(nntc_b200_device* d, nntc_b200_model* m, const nn
                 moved0 += l0[(size_t)p].moved_total;
         }
         r->ms_c += ms;
-        NB_TRY(objective(ec));
+        if (a->form == 1 && d->mixed_gram)
+        {
+            double t = 0.0;
+            NB_TRY(nb::normal_equations_and_objective(d, m, k, per_site, &ec, &t));
+            r->ms_a += t;
+            prepared = true;
+        }
+        else
+            NB_TRY(objective(ec));
         (void)E_REL;
         (void)E_NOISE;
         r->rounds_used = round;

@@ -76,12 +76,23 @@ constexpr uint32_t TG_SHARED = TG_ACC_OFFSET + TG_ACC_BYTES > TG_REACH ? TG_ACC_
 static_assert(TG_SHARED <= 56 * 1024, "four CTAs per SM");
 static_assert(TG_ACC_OFFSET % 16 == 0 && TG_BUF % 16 == 0, "16-byte aligned operand and accumulator regions");
 
+// The decoder for the objective the accumulation can form on the way (its own rows of Z are the sites' features and
+// targets): each output row at a fixed stride of 24, [c (4)][s (4)][s c (4 x 4)], as the FP32 objective lays it out.
+struct TcObjective
+{
+    float w[MAX_NOUT * 24];
+    float b[MAX_NOUT];
+    float cw[MAX_NOUT];
+    double* partial;        // [plane][3][LS_GRID]: sum cw e^2, the centre sites' sum e^2, the fractional sites'
+};
+
 struct TcArgs
 {
     double* partial;        // [plane][entry][LS_GRID]
     int entries;
     unsigned int* status;   // raised on a wait that gave up
     SiteTargetView tgt;
+    TcObjective obj;        // read only by the OBJ instantiation
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -176,7 +187,11 @@ __device__ __forceinline__ void tc_readback(uint32_t tmem, int warp, int lane, d
     }
 }
 
-template <int NOUT>
+// OBJ: also E of the decoder in A.obj at the same sites - the FP32 objective's decode and sums (k_objective_f32's
+// arithmetic, its fused multiply-adds in its order), each site's squared residuals summed in FP32, the sites' sums per
+// thread in FP64, one partial per CTA - so that the round's closing objective pass and the next round's normal
+// equations, which read the same sites at the same latents, are one pass.
+template <int NOUT, bool OBJ>
 __global__ void __launch_bounds__(TG_THREADS, 4) k_ls_accumulate_tc(Planes P, const __grid_constant__ TcArgs A)
 {
     extern __shared__ __align__(1024) unsigned char tg_sh[];
@@ -193,6 +208,7 @@ __global__ void __launch_bounds__(TG_THREADS, 4) k_ls_accumulate_tc(Planes P, co
     const long long chunks = (texels + TG_THREADS - 1) / TG_THREADS;
     const float* tgt = A.tgt.t + (size_t)A.tgt.site0[pl] * NOUT;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double e_weighted = 0.0, e_centre = 0.0, e_fractional = 0.0;   // OBJ: this thread's sites' sums
 
     for (int i = tid; i < 2 * TG_ROWS * TG_ACC_STRIDE; i += TG_THREADS)
         acc[i] = 0.0;
@@ -276,6 +292,32 @@ __global__ void __launch_bounds__(TG_THREADS, 4) k_ls_accumulate_tc(Planes P, co
                 if (valid)
                 {
                     site_z<NOUT>(P, V, tgt, pixel, px, py, j, z);
+                    if constexpr (OBJ)
+                    {
+                        float sw = 0.0f, ss = 0.0f;
+#pragma unroll
+                        for (int r = 0; r < NOUT; r++)
+                        {
+                            float acc = A.obj.b[r];
+#pragma unroll
+                            for (int h = 0; h < 4; h++)
+                                acc = __fmaf_rn(A.obj.w[r * 24 + h], z[ZS_C + h], acc);
+#pragma unroll
+                            for (int h = 0; h < 4; h++)
+                                acc = __fmaf_rn(A.obj.w[r * 24 + 4 + h], z[ZS_S + h], acc);
+#pragma unroll
+                            for (int h = 0; h < 16; h++)
+                                acc = __fmaf_rn(A.obj.w[r * 24 + 8 + h], z[ZS_SC + h], acc);
+                            const float e = acc - z[ZS_T + r];
+                            sw = __fmaf_rn(A.obj.cw[r] * e, e, sw);
+                            ss = __fmaf_rn(e, e, ss);
+                        }
+                        e_weighted += (double)sw;
+                        if (j == 0)
+                            e_centre += (double)ss;
+                        else
+                            e_fractional += (double)ss;
+                    }
 #pragma unroll
                     for (int q = 0; q < ZS_WIDTH; q += 4)
                     {
@@ -417,18 +459,68 @@ __global__ void __launch_bounds__(TG_THREADS, 4) k_ls_accumulate_tc(Planes P, co
         }
         A.partial[((size_t)pl * A.entries + e) * LS_GRID + blockIdx.x] = g;
     }
+    if constexpr (OBJ)
+    {
+        // the CTA's three objective sums: each warp's in lane order, then the four warps' in warp order
+        __shared__ double ored[3][TG_THREADS / 32];
+        double v[3] = { e_weighted, e_centre, e_fractional };
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+        {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+            if (lane == 0)
+                ored[q][warp] = v[q];
+        }
+        __syncthreads();
+        if (tid < 3)
+        {
+            double t = 0.0;
+            for (int w = 0; w < TG_THREADS / 32; w++)
+                t += ored[tid][w];
+            A.obj.partial[((size_t)pl * 3 + tid) * LS_GRID + blockIdx.x] = t;
+        }
+    }
 }
 
 int launch_ls_accumulate_tc(nntc_b200_device* d, const Planes& P, double* partial, int entries,
-                            const SiteTargetView& tgt, cudaStream_t stream)
+                            const SiteTargetView& tgt, cudaStream_t stream, double* obj_partial)
 {
     dim3 grid(LS_GRID, (unsigned)P.n);
-    const TcArgs args{ partial, entries, d->counters + CNT_STATUS, tgt };
+    TcArgs args{ partial, entries, d->counters + CNT_STATUS, tgt, {} };
+    if (obj_partial)
+    {
+        // the decoder as uploaded, in the objective's row layout
+        const int nin = d->nin, c0 = d->c0, c1 = d->c1;
+        for (int r = 0; r < d->nout; r++)
+        {
+            for (int q = 0; q < c1; q++)
+                args.obj.w[r * 24 + q] = d->host_weights[(size_t)r * nin + q];
+            for (int i = 0; i < c0; i++)
+                args.obj.w[r * 24 + 4 + i] = d->host_weights[(size_t)r * nin + c1 + i];
+            for (int i = 0; i < c0; i++)
+                for (int q = 0; q < c1; q++)
+                    args.obj.w[r * 24 + 8 + i * 4 + q] = d->host_weights[(size_t)r * nin + c1 + c0 + i * c1 + q];
+            args.obj.b[r] = d->host_bias[r];
+            args.obj.cw[r] = d->m.cw[r];
+        }
+        args.obj.partial = obj_partial;
+    }
 #define NB_TC(NO)                                                                                                     \
     case NO:                                                                                                          \
-        NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_tc<NO>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
-                                     (int)TG_SHARED));                                                                \
-        k_ls_accumulate_tc<NO><<<grid, TG_THREADS, TG_SHARED, stream>>>(P, args);                                     \
+        if (obj_partial)                                                                                              \
+        {                                                                                                             \
+            NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_tc<NO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                         (int)TG_SHARED));                                                            \
+            k_ls_accumulate_tc<NO, true><<<grid, TG_THREADS, TG_SHARED, stream>>>(P, args);                           \
+        }                                                                                                             \
+        else                                                                                                          \
+        {                                                                                                             \
+            NB_CUDA(cudaFuncSetAttribute(k_ls_accumulate_tc<NO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)TG_SHARED));                                                            \
+            k_ls_accumulate_tc<NO, false><<<grid, TG_THREADS, TG_SHARED, stream>>>(P, args);                          \
+        }                                                                                                             \
         break;
     switch (d->nout)
     {

@@ -30,7 +30,7 @@ namespace nb
 
 int assemble(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0, bool diag_only);
 int descent_direction(nntc_b200_device* d, const nntc_b200_model* m, int k, double ridge, int level0);
-int normal_equations(nntc_b200_device* d, int k, const double* per_site, double* ms);
+int normal_equations(nntc_b200_device* d, int k, const double* per_site, double* ms, std::vector<double>* obj_sums);
 
 // v = prev + alpha z, then onto the grid (bits, lo, hi) with its index when `snap`.
 __global__ void k_joint_apply(Planes P, float alpha, int snap, int bits, const float* lo, const float* hi)
@@ -122,7 +122,7 @@ extern "C" int nntc_b200_objective_gradient(nntc_b200_device* d, const nntc_b200
     if (g_dec)
     {
         double t = 0.0;
-        NB_TRY(normal_equations(d, k, per_site, &t));
+        NB_TRY(normal_equations(d, k, per_site, &t, nullptr));
         const int nin = m->nin, nout = m->nout, mm = nin + 1, tri = mm * (mm + 1) / 2;
         std::vector<double> ne((size_t)(tri + nout * mm));
         NB_TRY(download(d, ne.data(), d->reduction, ne.size() * sizeof(double)));

@@ -575,6 +575,14 @@ static void normalise(const nntc_b200_model& m, int k, const double* per_site, c
     r->sampled_mse = k > 0 ? acc[2] / (base * (double)k) : 0.0;
 }
 
+// The reported numbers from three raw sums per plane formed elsewhere (the tensor-core normal equations' pass).
+void objective_from_sums(const nntc_b200_model& m, int k, const double* per_site, const std::vector<double>& acc,
+                         nntc_b200_objective* r)
+{
+    *r = nntc_b200_objective{};
+    normalise(m, k, per_site, acc, r);
+}
+
 static double g_objective_ms = 0.0;
 static long long g_objective_calls = 0;
 
