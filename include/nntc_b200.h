@@ -396,6 +396,11 @@ int nntc_b200_probe_source(nntc_b200_device* d, int plane, float* out, size_t n)
 int nntc_b200_probe_jtj_level1(nntc_b200_device* d, int k, int plane, const double* x, double* y, size_t n);
 /* The same for block (c')'s operator over level 0 (src/solve_level1.cu:440-581): x and y w0 h0 c0 doubles; bc8 only. */
 int nntc_b200_probe_jtj_level0(nntc_b200_device* d, int k, int plane, const double* x, double* y, size_t n);
+/* The adjoint form's round-closing pass (no counterpart in the reference, whose objective and normal equations are
+ * separate passes): block (a)'s normal equations on the tensor cores (left where nntc_b200_probe_normal_equations reads
+ * them) and E of the uploaded decoder at the same sites, in one pass. Needs NNTC_B200_OPT_MIXED_PRECISION_GRAM on. */
+int nntc_b200_probe_objective_with_normal_equations(nntc_b200_device* d, const nntc_b200_model* m, int k,
+                                                    const double* per_site, nntc_b200_objective* r);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,7 @@ PROTOTYPES = {
     "nntc_b200_objective_gradient": (_I, [_P, _M, _I, _PD, _PPD, _PPD, _PD]),
     "nntc_b200_measure_fma_peaks": (_I, [_PD, _PD]),
     "nntc_b200_probe_normal_equations": (_I, [_P, _PD, _S]),
+    "nntc_b200_probe_objective_with_normal_equations": (_I, [_P, _P, _I, _PD, _P]),
     "nntc_b200_probe_workspace": (_I, [_P, _I, _I, _PD, _PD, _PF, _PD, _PF]),
     "nntc_b200_probe_monomials": (_I, [_P, _I, _PD, _S]),
     "nntc_b200_probe_source": (_I, [_P, _I, _PF, _S]),

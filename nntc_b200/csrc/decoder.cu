@@ -628,6 +628,18 @@ int solve_decoder_prepared(nntc_b200_device* d, nntc_b200_model* m, int k, const
 extern "C"
 {
 
+int nntc_b200_probe_objective_with_normal_equations(nntc_b200_device* d, const nntc_b200_model* m, int k,
+                                                    const double* per_site, nntc_b200_objective* r)
+{
+    if (!d->mixed_gram)
+    {
+        set_error(NNTC_B200_ERR_STATE, "the objective rides only on the tensor-core normal equations");
+        return NNTC_B200_ERR_STATE;
+    }
+    double ms = 0.0;
+    return normal_equations_and_objective(d, m, k, per_site, r, &ms);
+}
+
 void nntc_b200_decoder_ridge_tally(long long out[4])
 {
     for (int i = 0; i < 4; i++)

@@ -122,3 +122,33 @@ def test_fp32_stencil_vs_fp64(textures, c0, c1, w, h):
                     scale = np.abs(a[key]).max()
                     err = np.abs(b[key] - a[key]).max()
                     assert err <= 1e-5 * scale, (level0, i, key, err / max(scale, 1e-300))
+
+
+@pytest.mark.parametrize("textures,c0,c1,w,h,k", [(4, 4, 4, 128, 96, 4), (6, 4, 4, 70, 52, 4), (2, 2, 4, 64, 48, 2)])
+def test_objective_with_normal_equations(textures, c0, c1, w, h, k):
+    """The adjoint form's round-closing pass (the tensor-core normal equations and E of the current decoder from one
+    pass over the sites) against the two passes it replaces, on the same state: the normal equations the same bits as
+    the tensor-core pass alone, E and every plane's E within 1e-12 of the FP32 objective (the same per-site values,
+    their FP64 sums in another order)."""
+    mat, v0, v1 = state(w * h + 13 * textures, w, h, textures, c0, c1, k)
+    rng = np.random.default_rng(w + 2 * h)
+    nin, nout = abi.feature_count(c0, c1), 3 * textures
+    with Session(mat) as s:
+        for i in range(len(mat.planes)):
+            s.set_planes(i, v0[i], v1[i])
+        s.set_decoder(rng.standard_normal((nout, nin)) * 0.2, rng.random(nout) * 0.5)
+        for opt in (abi.OPT_MIXED_PRECISION_GRAM, abi.OPT_MIXED_OBJECTIVE):
+            check(lib().nntc_b200_set_option(s.d, opt, 1), "option")
+        ref = s.objective(k)
+        w_keep, b_keep = s.decoder()
+        s.solve_decoder(k)                      # the tensor-core normal equations alone (and a solve)
+        ne_alone = s.normal_equations()
+        s.set_decoder(w_keep, b_keep)
+        got = abi.Objective()
+        check(lib().nntc_b200_probe_objective_with_normal_equations(s.d, C.byref(s.m), k, s.per_site, C.byref(got)),
+              "fused")
+        ne_fused = s.normal_equations()
+    assert np.array_equal(ne_fused, ne_alone)
+    assert abs(got.e - ref.e) <= 1e-12 * ref.e, (got.e, ref.e)
+    for i in range(len(mat.planes)):
+        assert abs(got.e_plane[i] - ref.e_plane[i]) <= 1e-12 * ref.e_plane[i], (i, got.e_plane[i], ref.e_plane[i])
