@@ -33,7 +33,7 @@ namespace nb
 
 constexpr int SITE_THREADS = 256;
 constexpr int GATHER_THREADS = 128;
-constexpr int GATHER_RING = 6;   // visits in flight per thread on the interior walk (cp.async into shared memory)
+constexpr int GATHER_RING = 4;   // visits in flight per thread on the interior walk (cp.async into shared memory)
 
 // One visit's operands, staged by cp.async: the site's sample of the other latent and (self slot) its gradient term.
 struct __align__(16) VisitSlot
@@ -624,7 +624,7 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
 
     // the slot's block, expanded once against the monomial matrices in the reference's order (src/solve_level1.cu:382-399);
     // level 1 expands it in two halves of eight entries (each entry's own sum still in monomial order) so that fewer
-    // doubles are live at once and six blocks (as many as the visit rings' shared memory allows) fit an SM
+    // doubles are live at once and six blocks (FP64) or eight (FP32) fit an SM
     // (where the gradient's store goes changes only which registers are live when: each level's place is the one that
     // spills least at its occupancy)
     auto store_grad = [&]() {
@@ -685,8 +685,8 @@ __device__ __forceinline__ void gather_body(const Planes& P, const GatherArgs& A
         store_grad();
 }
 
-// The two levels' kernels: level 1 capped at six blocks per SM (its expansion is split for that; the visit rings'
-// shared memory allows six); level 0's FP64 gather left at the register count it takes (a cap made it spill and run
+// The two levels' kernels: level 1's FP64 gather capped at six blocks per SM (its expansion is split for that), its
+// FP32 gather at eight (64 registers; the visit rings' shared memory allows nine); level 0's FP64 gather left at the register count it takes (a cap made it spill and run
 // slower), its FP32 gather at eight blocks per SM (64 registers, no spills: 18.4 -> 17.7 ms per assembly).
 template <typename TS>
 __global__ void __launch_bounds__(GATHER_THREADS, (sizeof(TS) == sizeof(float) ? 8 : 1)) k_gather_level0(Planes P, const __grid_constant__ GatherArgs A)
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(GATHER_THREADS, (sizeof(TS) == sizeof(float) ?
 }
 
 template <typename TS>
-__global__ void __launch_bounds__(GATHER_THREADS, 6) k_gather_level1(Planes P, const __grid_constant__ GatherArgs A)
+__global__ void __launch_bounds__(GATHER_THREADS, (sizeof(TS) == sizeof(float) ? 8 : 6)) k_gather_level1(Planes P, const __grid_constant__ GatherArgs A)
 {
     gather_body<false, TS>(P, A);
 }
