@@ -538,14 +538,33 @@ template <int PASS>
 __global__ void k_residual_pass(ResidualRows R, size_t texels, Basis* B, ResidualPassArgs a)
 {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (PASS == RP_PEAK)
+    {
+        // the largest |projection|: each warp's maximum first (a maximum is the same whatever the order), then one
+        // atomic per warp - one per texel had every texel of the chain contend for one address
+        unsigned long long bits = 0ull;   // |p| >= 0: the bits order as the values
+        if (t < texels)
+        {
+            float row[MAX_NOUT];
+            R.row(t, row);
+            bits = (unsigned long long)__double_as_longlong(fabs(project(row, *B, 0, R.nout)));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, bits, o);
+            bits = x > bits ? x : bits;
+        }
+        if ((threadIdx.x & 31) == 0 && bits != 0ull)
+            atomicMax(&B->peak_bits[0], bits);
+        return;
+    }
     if (t >= texels)
         return;
     float row[MAX_NOUT];
     R.row(t, row);
     const double p = project(row, *B, 0, R.nout);
-    if (PASS == RP_PEAK)
-        peak_max(&B->peak_bits[0], fabs(p));
-    else if (PASS == RP_HIST)
+    if (PASS == RP_HIST)
     {
         const double peak = __longlong_as_double((long long)B->peak_bits[0]);
         if (!(peak > 0.0))
